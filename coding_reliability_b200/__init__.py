@@ -1,0 +1,293 @@
+"""B200-native distance-distribution histograms (AN codes, Extended Hamming).
+
+Python host-side mirror of the C-ABI in include/codrel_b200.h.  The compute
+always runs in libcodrel_b200.so on the GPU; there is no Python or CPU
+fallback: loading fails loudly if the library is missing, and every call that
+needs a device raises when none is present.
+
+The reference's driver names are mirrored by thin functions (run_ancoding,
+run_ancoding_grid, run_ancoding_mc, run_hamming, run_hamming_grid,
+run_hamming_mc; distance_distribution/src/algorithms.h:20-34) that return the
+post-processed uint128 counts[] as Python ints.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass, field
+from pathlib import Path
+
+__all__ = [
+    "CODE_AN", "CODE_EXT_HAMMING", "MODE_EXHAUSTIVE", "MODE_GRID_1D", "MODE_GRID_2D", "MODE_MONTE_CARLO",
+    "KERNEL_AUTO", "KERNEL_POPC", "KERNEL_MMA", "HAMMING_WEIGHTS", "HAMMING_ALL_PAIRS", "HAMMING_ALL_PAIRS_DISTINCT",
+    "CONV_GPU", "CONV_CPU", "CONV_SUPER_A", "MAX_BINS", "DDError", "Request", "Result", "Context",
+    "load", "lib_path", "postprocess", "format_result", "request_shape", "philox4x32_10", "device_count",
+    "run_ancoding", "run_ancoding_cpu", "run_ancoding_grid", "run_ancoding_mc", "run_hamming",
+    "run_hamming_grid", "run_hamming_mc",
+]
+
+CODE_AN, CODE_EXT_HAMMING = 0, 1
+MODE_EXHAUSTIVE, MODE_GRID_1D, MODE_GRID_2D, MODE_MONTE_CARLO = 0, 1, 2, 3
+KERNEL_AUTO, KERNEL_POPC, KERNEL_MMA = 0, 1, 2
+HAMMING_WEIGHTS, HAMMING_ALL_PAIRS, HAMMING_ALL_PAIRS_DISTINCT = 0, 1, 2
+CONV_GPU, CONV_CPU, CONV_SUPER_A = 0, 1, 2
+MAX_BINS = 64
+
+STATUS = {
+    0: "ok", 1: "invalid argument", 2: "unsupported", 3: "cuda error", 4: "no device",
+    5: "out of memory", 6: "busy", 7: "timeout", 8: "not found", 9: "cancelled",
+}
+
+_PKG = Path(__file__).resolve().parent
+
+
+def lib_path() -> Path:
+    return Path(os.environ.get("CODREL_B200_LIB", _PKG / "libcodrel_b200.so"))
+
+
+class DDError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"{STATUS.get(status, status)}: {msg}")
+        self.status = status
+
+
+class _Req(C.Structure):
+    _fields_ = [("code", C.c_uint32), ("mode", C.c_uint32), ("A", C.c_uint64), ("n", C.c_uint32),
+                ("h", C.c_uint32), ("m", C.c_uint64), ("m2", C.c_uint64), ("seed", C.c_uint64),
+                ("with_1bit", C.c_uint32), ("hamming_method", C.c_uint32), ("kernel", C.c_uint32),
+                ("convention", C.c_uint32), ("user_tag", C.c_uint64)]
+
+
+class _Res(C.Structure):
+    _fields_ = [("status", C.c_uint32), ("nbins", C.c_uint32), ("h", C.c_uint32), ("kernel_used", C.c_uint32),
+                ("A", C.c_uint64), ("iterations", C.c_uint64), ("iterations2", C.c_uint64),
+                ("pairs_lo", C.c_uint64), ("pairs_hi", C.c_uint64),
+                ("raw", C.c_uint64 * MAX_BINS), ("counts_lo", C.c_uint64 * MAX_BINS),
+                ("counts_hi", C.c_uint64 * MAX_BINS), ("minb", C.c_uint64), ("mincb_lo", C.c_uint64),
+                ("mincb_hi", C.c_uint64), ("max_rel_error", C.c_double), ("kernel_ms", C.c_double),
+                ("total_ms", C.c_double), ("user_tag", C.c_uint64)]
+
+
+class _BatchOpts(C.Structure):
+    _fields_ = [("use_graph", C.c_uint32), ("kernel", C.c_uint32), ("ctas_per_sm", C.c_uint32),
+                ("reserved", C.c_uint32)]
+
+
+@dataclass
+class Request:
+    code: int = CODE_AN
+    mode: int = MODE_EXHAUSTIVE
+    A: int = 61
+    n: int = 8
+    h: int = 0
+    m: int = 0
+    m2: int = 0
+    seed: int = 0
+    with_1bit: int = 0
+    hamming_method: int = HAMMING_WEIGHTS
+    kernel: int = KERNEL_AUTO
+    convention: int = CONV_GPU
+    user_tag: int = 0
+
+    def _c(self) -> _Req:
+        return _Req(self.code, self.mode, self.A, self.n, self.h, self.m, self.m2, self.seed, self.with_1bit,
+                    self.hamming_method, self.kernel, self.convention, self.user_tag)
+
+
+@dataclass
+class Result:
+    nbins: int
+    h: int
+    A: int
+    raw: list[int]
+    counts: list[int]
+    minb: int
+    mincb: int
+    max_rel_error: float
+    kernel_ms: float
+    total_ms: float
+    pairs: int
+    iterations: int
+    iterations2: int
+    kernel_used: int
+    user_tag: int = 0
+    _c: object = field(default=None, repr=False)
+
+    @staticmethod
+    def _from(r: _Res) -> "Result":
+        nb = r.nbins
+        return Result(
+            nbins=nb, h=r.h, A=r.A, raw=[r.raw[i] for i in range(nb)],
+            counts=[(r.counts_hi[i] << 64) | r.counts_lo[i] for i in range(nb)],
+            minb=r.minb, mincb=(r.mincb_hi << 64) | r.mincb_lo, max_rel_error=r.max_rel_error,
+            kernel_ms=r.kernel_ms, total_ms=r.total_ms, pairs=(r.pairs_hi << 64) | r.pairs_lo,
+            iterations=r.iterations, iterations2=r.iterations2, kernel_used=r.kernel_used,
+            user_tag=r.user_tag, _c=r)
+
+
+_lib = None
+
+
+def load() -> C.CDLL:
+    """Loads libcodrel_b200.so; raises if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    p = lib_path()
+    if not p.exists():
+        raise RuntimeError(f"{p} is missing: build it with `python -m coding_reliability_b200.build`")
+    lib = C.CDLL(str(p))
+    vp, i32, u32 = C.c_void_p, C.c_int, C.c_uint32
+    lib.dd_version.restype = C.c_char_p
+    lib.dd_status_string.restype = C.c_char_p
+    lib.dd_last_error.restype = C.c_char_p
+    lib.dd_device_count.restype = i32
+    lib.dd_context_create.argtypes = [i32, vp, C.POINTER(vp)]
+    lib.dd_context_destroy.argtypes = [vp]
+    lib.dd_histogram.argtypes = [vp, C.POINTER(_Req), C.POINTER(_Res)]
+    lib.dd_batch_run.argtypes = [vp, C.POINTER(_Req), u32, C.POINTER(_Res), C.POINTER(_BatchOpts)]
+    lib.dd_request_shape.argtypes = [C.POINTER(_Req), C.POINTER(u32), C.POINTER(u32), C.POINTER(C.c_uint64)]
+    lib.dd_postprocess.argtypes = [C.POINTER(_Req), C.POINTER(C.c_uint64), u32, C.POINTER(_Res)]
+    lib.dd_format_result.argtypes = [C.POINTER(_Req), C.POINTER(_Res), C.c_char_p, C.c_char_p, C.c_size_t,
+                                     C.POINTER(C.c_size_t)]
+    lib.dd_philox4x32_10.argtypes = [C.POINTER(u32), C.POINTER(u32), C.POINTER(u32)]
+    lib.dd_philox4x32_10.restype = None
+    lib.dd_measure_popc_peak.argtypes = [vp, C.POINTER(C.c_double)]
+    _lib = lib
+    return lib
+
+
+def _check(st: int) -> None:
+    if st != 0:
+        raise DDError(st, load().dd_last_error().decode())
+
+
+def device_count() -> int:
+    return load().dd_device_count()
+
+
+def request_shape(req: Request) -> tuple[int, int, int]:
+    nb, h, a = C.c_uint32(), C.c_uint32(), C.c_uint64()
+    _check(load().dd_request_shape(C.byref(req._c()), C.byref(nb), C.byref(h), C.byref(a)))
+    return nb.value, h.value, a.value
+
+
+def postprocess(req: Request, raw: list[int]) -> Result:
+    """The reference drivers' host post-processing of a raw histogram (no device needed)."""
+    arr = (C.c_uint64 * MAX_BINS)(*([int(x) for x in raw] + [0] * (MAX_BINS - len(raw))))
+    out = _Res()
+    _check(load().dd_postprocess(C.byref(req._c()), arr, MAX_BINS, C.byref(out)))
+    return Result._from(out)
+
+
+def format_result(req: Request, res: Result, device_line: str | None = None) -> str:
+    lib = load()
+    n = C.c_size_t()
+    r = res._c if res._c is not None else _Res()
+    dl = device_line.encode() if device_line is not None else None
+    _check(lib.dd_format_result(C.byref(req._c()), C.byref(r), dl, None, 0, C.byref(n)))
+    buf = C.create_string_buffer(n.value + 1)
+    _check(lib.dd_format_result(C.byref(req._c()), C.byref(r), dl, buf, n.value + 1, C.byref(n)))
+    return buf.value.decode()
+
+
+def philox4x32_10(ctr: tuple[int, int, int, int], key: tuple[int, int]) -> tuple[int, int, int, int]:
+    c = (C.c_uint32 * 4)(*ctr)
+    k = (C.c_uint32 * 2)(*key)
+    o = (C.c_uint32 * 4)()
+    load().dd_philox4x32_10(c, k, o)
+    return tuple(o)
+
+
+class Context:
+    """One device + one CUDA stream (dd_context)."""
+
+    def __init__(self, device: int = 0, stream: int | None = None):
+        lib = load()
+        h = C.c_void_p()
+        _check(lib.dd_context_create(device, C.c_void_p(stream) if stream else None, C.byref(h)))
+        self._h = h
+        self.device = device
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            load().dd_context_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def histogram(self, req: Request) -> Result:
+        out = _Res()
+        _check(load().dd_histogram(self._h, C.byref(req._c()), C.byref(out)))
+        return Result._from(out)
+
+    def batch(self, reqs: list[Request], use_graph: bool = True, kernel: int = KERNEL_AUTO) -> list[Result]:
+        n = len(reqs)
+        arr = (_Req * n)(*[r._c() for r in reqs])
+        out = (_Res * n)()
+        opts = _BatchOpts(1 if use_graph else 0, kernel, 0, 0)
+        _check(load().dd_batch_run(self._h, arr, n, out, C.byref(opts)))
+        return [Result._from(out[i]) for i in range(n)]
+
+    def popc_peak(self) -> float:
+        v = C.c_double()
+        _check(load().dd_measure_popc_peak(self._h, C.byref(v)))
+        return v.value
+
+
+_default_ctx: Context | None = None
+
+
+def _ctx() -> Context:
+    global _default_ctx
+    if _default_ctx is None:
+        _default_ctx = Context(0)
+    return _default_ctx
+
+
+# -- the reference's driver names -------------------------------------------------
+def run_ancoding(n: int, A: int) -> Result:
+    """src/an_coding.cu:276 run_ancoding (GPU conventions)."""
+    return _ctx().histogram(Request(CODE_AN, MODE_EXHAUSTIVE, A, n, convention=CONV_GPU))
+
+
+def run_ancoding_cpu(n: int, A: int) -> Result:
+    """src/an_coding.cpp:104 run_ancoding_cpu conventions, computed on the GPU."""
+    return _ctx().histogram(Request(CODE_AN, MODE_EXHAUSTIVE, A, n, convention=CONV_CPU))
+
+
+def run_ancoding_grid(gdim: int, n: int, m: int, m2: int, A: int) -> Result:
+    """src/an_coding_grid.cu:215 run_ancoding_grid."""
+    return _ctx().histogram(Request(CODE_AN, MODE_GRID_2D if gdim == 2 else MODE_GRID_1D, A, n, m=m, m2=m2))
+
+
+def run_ancoding_mc(n: int, m: int, A: int, seed: int = 16384) -> Result:
+    """src/an_coding_mc.cu:205 run_ancoding_mc (Philox draws)."""
+    return _ctx().histogram(Request(CODE_AN, MODE_MONTE_CARLO, A, n, m=m, seed=seed))
+
+
+def run_hamming(n: int, with_1bit: int = 0, method: int = HAMMING_WEIGHTS) -> Result:
+    """src/hamming.cu:97 run_hamming (`-e 1`) or the all-pairs brute force (`-e 2/3/4`)."""
+    return _ctx().histogram(Request(CODE_EXT_HAMMING, MODE_EXHAUSTIVE, 1, n, with_1bit=with_1bit,
+                                    hamming_method=method))
+
+
+def run_hamming_grid(n: int, with_1bit: int, m: int) -> Result:
+    """src/hamming_grid.cu:91 run_hamming_grid."""
+    return _ctx().histogram(Request(CODE_EXT_HAMMING, MODE_GRID_1D, 1, n, m=m, with_1bit=with_1bit))
+
+
+def run_hamming_mc(n: int, with_1bit: int, m: int, seed: int = 1337) -> Result:
+    """src/hamming_mc.cu:98 run_hamming_mc (Philox draws)."""
+    return _ctx().histogram(Request(CODE_EXT_HAMMING, MODE_MONTE_CARLO, 1, n, m=m, seed=seed,
+                                    with_1bit=with_1bit))

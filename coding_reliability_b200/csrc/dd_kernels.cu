@@ -1,0 +1,426 @@
+// dd_kernels.cu — the popc-path histogram kernels (sm_100a).
+//
+// One persistent kernel serves every job kind.  Each warp is an independent
+// worker: it claims a tile from a global counter, accumulates distances into
+// its own shared-memory bins (one uint32 column per lane, so increments never
+// collide), and flushes those bins warp-aggregated into the job's uint64
+// global bins when it moves to another job, every kFlushEvery tiles, and at
+// exit.  Codewords are generated in registers (A*x, lattice points, Hamming
+// parity), never read from HBM.
+//
+// Reference kernels this replaces (all plain SIMT, written for sm_35):
+//   dancoding_shared        distance_distribution/src/an_coding.cu:50-105
+//   dancoding_grid_1d_shared                       src/an_coding_grid.cu:60-114
+//   dancoding_grid_2d                              src/an_coding_grid.cu:121-140
+//   dancoding_mc_shared                            src/an_coding_mc.cu:94-158
+//   dhamming / dhamming_grid_1d / dhamming_mc      src/hamming.cu:64-81, hamming_grid.cu:53-74,
+//                                                  hamming_mc.cu:57-81
+//   super-A dancoding_shared / dancoding           distance_distribution_super_a/src/an_coding.cu:32-99
+#include <cuda_runtime.h>
+#include <cstdint>
+
+#include "dd_device.cuh"
+#include "dd_jobs.h"
+#include "dd_kernels.h"
+
+namespace dd {
+
+// ---------------------------------------------------------------------------
+// shared-memory bin increments
+// ---------------------------------------------------------------------------
+template <int kMode>
+__device__ __forceinline__ void bump(uint32_t saddr) {
+  if constexpr (kMode == HIST_RED) {
+    asm volatile("red.shared.add.u32 [%0], 1;" ::"r"(saddr) : "memory");
+  } else {
+    uint32_t v;
+    asm volatile("ld.shared.u32 %0, [%1];" : "=r"(v) : "r"(saddr) : "memory");
+    asm volatile("st.shared.u32 [%0], %1;" ::"r"(saddr), "r"(v + 1) : "memory");
+  }
+}
+
+// Warp-aggregated flush: lane l sums bin rows l and l+32 over the 32 lane
+// columns (rotated so the 32 lanes hit 32 different banks), zeroes them and
+// adds the 64-bit sums to the global bins.
+__device__ __forceinline__ void flush_bins(uint32_t* wbins, unsigned long long* gbins, uint32_t nbins, int lane) {
+  __syncwarp();
+  for (uint32_t b = lane; b < nbins; b += 32) {
+    unsigned long long s = 0;
+#pragma unroll 8
+    for (int k = 0; k < 32; ++k) {
+      const int kk = (k + lane) & 31;
+      s += wbins[b * 32 + kk];
+      wbins[b * 32 + kk] = 0;
+    }
+    if (s) atomicAdd(gbins + b, s);
+  }
+  __syncwarp();
+}
+
+// ---------------------------------------------------------------------------
+// generators
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint64_t lattice_value(uint64_t A, uint64_t k, double step, uint32_t t32) {
+  // v = A * (T)(k * stepsize), T = uint32 or uint64 as the reference's Caller picks it.
+  if (t32) return (uint64_t)(uint32_t)(A * (uint64_t)(uint32_t)((double)k * step));
+  return A * (uint64_t)((double)k * step);
+}
+
+__device__ __forceinline__ uint64_t row_value(const Job& J, uint64_t i) {
+  switch (J.row_kind) {
+    case ROW_LATTICE: return lattice_value(J.A, i, J.row_step, J.t32);
+    case ROW_HAMMING_EXT: return hamming_cw_ext(i, J.n);
+    default: return J.A * i;
+  }
+}
+
+__device__ __forceinline__ uint64_t col_value(const Job& J, uint64_t j) {
+  switch (J.col_kind) {
+    case COL_LATTICE: return lattice_value(J.A, j, J.col_step, J.t32);
+    case COL_HAMMING_EXT: return hamming_cw_ext(j, J.n);
+    default: return J.A * j;
+  }
+}
+
+// Upper-triangle decode: s in [0, M(M+1)/2) -> (r, c), r <= c, row-major.
+__device__ __forceinline__ void tri_decode(uint64_t s, uint64_t M, uint64_t& r, uint64_t& c) {
+  const double b = 2.0 * (double)M + 1.0;
+  double disc = b * b - 8.0 * (double)s;
+  if (disc < 0) disc = 0;
+  int64_t rr = (int64_t)((b - sqrt(disc)) * 0.5);
+  if (rr < 0) rr = 0;
+  if ((uint64_t)rr >= M) rr = (int64_t)M - 1;
+  auto S = [M](uint64_t r_) { return r_ * M - (r_ * (r_ - (r_ ? 1 : 0))) / 2; };
+  // S(r) = r*M - r*(r-1)/2 entries precede row r
+  while ((uint64_t)rr + 1 < M && S((uint64_t)rr + 1) <= s) ++rr;
+  while (rr > 0 && S((uint64_t)rr) > s) --rr;
+  r = (uint64_t)rr;
+  c = r + (s - S(r));
+}
+
+// ---------------------------------------------------------------------------
+// pair tiles
+// ---------------------------------------------------------------------------
+
+// Fast path: 32 lanes x kRowsPerLane valid rows, columns [c, ce) an arithmetic
+// progression v = A*j with warp-uniform v; `off[q]` is the shared address of
+// lane's bin 0 for row q, already shifted by the high-word distance.
+template <int kMode>
+__device__ __forceinline__ void run_progression(const uint32_t (&w)[kRowsPerLane], const uint32_t (&off)[kRowsPerLane],
+                                                uint32_t v, uint32_t a, uint32_t count) {
+  uint32_t j = 0;
+  for (; j + 8 <= count; j += 8) {
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+#pragma unroll
+      for (int q = 0; q < kRowsPerLane; ++q) bump<kMode>(off[q] + (__popc(w[q] ^ v) << 7));
+      v += a;
+    }
+  }
+  for (; j < count; ++j) {
+#pragma unroll
+    for (int q = 0; q < kRowsPerLane; ++q) bump<kMode>(off[q] + (__popc(w[q] ^ v) << 7));
+    v += a;
+  }
+}
+
+// Columns read from a per-warp table in shared memory (Ext-Hamming codewords).
+template <int kMode>
+__device__ __forceinline__ void run_table(const uint32_t (&w)[kRowsPerLane], const uint32_t (&off)[kRowsPerLane],
+                                          const uint32_t* table, uint32_t count) {
+  uint32_t j = 0;
+  for (; j + 4 <= count; j += 4) {
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const uint32_t v = table[j + u];
+#pragma unroll
+      for (int q = 0; q < kRowsPerLane; ++q) bump<kMode>(off[q] + (__popc(w[q] ^ v) << 7));
+    }
+  }
+  for (; j < count; ++j) {
+    const uint32_t v = table[j];
+#pragma unroll
+    for (int q = 0; q < kRowsPerLane; ++q) bump<kMode>(off[q] + (__popc(w[q] ^ v) << 7));
+  }
+}
+
+// Slow path for diagonal and partial tiles and for generic 64-bit columns:
+// every pair checked, 64-bit popcount.
+template <int kMode>
+__device__ __forceinline__ void run_generic(const Job& J, const uint64_t (&w)[kRowsPerLane],
+                                            const uint64_t (&ri)[kRowsPerLane], const bool (&rv)[kRowsPerLane],
+                                            uint32_t lane_base, uint64_t c0, uint64_t c1, bool diag) {
+  for (uint64_t j = c0; j < c1; ++j) {
+    const uint64_t v = col_value(J, j);
+#pragma unroll
+    for (int q = 0; q < kRowsPerLane; ++q)
+      if (rv[q] && (!diag || j > ri[q])) bump<kMode>(lane_base + (popc64(w[q] ^ v) << 7));
+  }
+}
+
+template <int kMode>
+__device__ void pairs_tile(const Job& J, uint64_t lt, uint32_t* wbins, uint32_t* table, int lane) {
+  uint64_t r0, c0, c1;
+  bool diag = false;
+  if (J.shape == SHAPE_TRIANGLE) {
+    const uint64_t s = lt / kStrips;
+    const uint32_t strip = (uint32_t)(lt % kStrips);
+    uint64_t sr, sc;
+    tri_decode(s, J.col_tiles, sr, sc);
+    r0 = sr * kSuper + (uint64_t)strip * kWarpRows;
+    c0 = sc * kSuper;
+    c1 = c0 + kSuper < J.cols ? c0 + kSuper : J.cols;
+    diag = (sr == sc);
+  } else {
+    const uint64_t rt = lt / J.col_tiles, ct = lt % J.col_tiles;
+    r0 = rt * kWarpRows;
+    c0 = ct * kTileCols;
+    c1 = c0 + kTileCols < J.cols ? c0 + kTileCols : J.cols;
+  }
+  if (r0 >= J.rows) return;
+
+  uint64_t w[kRowsPerLane], ri[kRowsPerLane];
+  bool rv[kRowsPerLane];
+  bool all_valid = true;
+#pragma unroll
+  for (int q = 0; q < kRowsPerLane; ++q) {
+    ri[q] = r0 + (uint64_t)q * 32 + lane;
+    rv[q] = ri[q] < J.rows;
+    all_valid &= rv[q];
+    w[q] = rv[q] ? row_value(J, ri[q]) : 0;
+  }
+  all_valid = __all_sync(0xffffffffu, all_valid);
+  const uint32_t lane_base = (uint32_t)__cvta_generic_to_shared(wbins) + (uint32_t)lane * 4u;
+
+  // Diagonal tile: columns <= r0 pair with no row; (r0, r0+kWarpRows) need the
+  // j > i mask; the rest is a full rectangle.
+  uint64_t cf = c0;
+  if (diag) {
+    const uint64_t mlo = r0 + 1 > c0 ? r0 + 1 : c0;
+    const uint64_t mhi = r0 + kWarpRows < c1 ? r0 + kWarpRows : c1;
+    if (mlo < mhi) run_generic<kMode>(J, w, ri, rv, lane_base, mlo, mhi, true);
+    cf = mhi > mlo ? mhi : mlo;
+    if (cf < c0) cf = c0;
+  }
+  if (cf >= c1) return;
+
+  if (!all_valid || J.col_kind == COL_LATTICE || (J.wide && J.col_kind != COL_PROGRESSION) ||
+      (J.col_kind == COL_PROGRESSION && J.wide && (J.A >> 32))) {
+    run_generic<kMode>(J, w, ri, rv, lane_base, cf, c1, false);
+    return;
+  }
+
+  uint32_t wl[kRowsPerLane], off[kRowsPerLane];
+#pragma unroll
+  for (int q = 0; q < kRowsPerLane; ++q) wl[q] = (uint32_t)w[q];
+
+  if (J.col_kind == COL_HAMMING_EXT) {
+    const uint32_t cnt = (uint32_t)(c1 - cf);
+    for (uint32_t jj = lane; jj < cnt; jj += 32) table[jj] = (uint32_t)hamming_cw_ext(cf + jj, J.n);
+    __syncwarp();
+#pragma unroll
+    for (int q = 0; q < kRowsPerLane; ++q) off[q] = lane_base;
+    run_table<kMode>(wl, off, table, cnt);
+    __syncwarp();
+    return;
+  }
+
+  const uint32_t a = (uint32_t)J.A;
+  if (!J.wide) {
+#pragma unroll
+    for (int q = 0; q < kRowsPerLane; ++q) off[q] = lane_base;
+    run_progression<kMode>(wl, off, (uint32_t)(J.A * cf), a, (uint32_t)(c1 - cf));
+    return;
+  }
+  // Wide codewords: split the columns where the high word of A*j changes, so
+  // that each segment needs one 32-bit popcount per pair; the high-word
+  // distance of row q is folded into its bin offset.
+  uint32_t wh[kRowsPerLane];
+#pragma unroll
+  for (int q = 0; q < kRowsPerLane; ++q) wh[q] = (uint32_t)(w[q] >> 32);
+  uint64_t j = cf;
+  uint64_t v = J.A * j;
+  while (j < c1) {
+    const uint32_t vl = (uint32_t)v, vh = (uint32_t)(v >> 32);
+    const uint64_t to_wrap = ((1ull << 32) - vl + a - 1) / a;
+    const uint64_t je = j + to_wrap < c1 ? j + to_wrap : c1;
+#pragma unroll
+    for (int q = 0; q < kRowsPerLane; ++q) off[q] = lane_base + (__popc(wh[q] ^ vh) << 7);
+    run_progression<kMode>(wl, off, vl, a, (uint32_t)(je - j));
+    v += J.A * (je - j);
+    j = je;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Monte Carlo tiles: 32 codeword rows x kMcSamplesPerTile samples each.
+// ---------------------------------------------------------------------------
+template <int kMode>
+__device__ void mc_tile(const Job& J, uint64_t lt, uint32_t* wbins, int lane) {
+  const uint64_t chunks = (J.iters + kMcSamplesPerTile - 1) / kMcSamplesPerTile;
+  const uint64_t rt = lt / chunks, ch = lt % chunks;
+  const uint64_t i = rt * 32 + lane;
+  if (i >= J.rows) return;
+  const uint64_t t0 = ch * kMcSamplesPerTile;
+  const uint64_t t1 = t0 + kMcSamplesPerTile < J.iters ? t0 + kMcSamplesPerTile : J.iters;
+  const uint32_t lane_base = (uint32_t)__cvta_generic_to_shared(wbins) + (uint32_t)lane * 4u;
+  const uint64_t w = J.A * i;
+  const uint32_t k0 = (uint32_t)J.seed, k1 = (uint32_t)(J.seed >> 32);
+  const uint32_t i0 = (uint32_t)i, i1 = (uint32_t)(i >> 32);
+  if (J.n <= 32) {
+    const unsigned sh = 32 - J.n;
+    const uint32_t wl = (uint32_t)w, wh = (uint32_t)(w >> 32);
+    const uint32_t a = (uint32_t)J.A;
+    uint64_t t = t0;
+    // whole Philox blocks (t0 is a multiple of 4)
+    for (; t + 4 <= t1; t += 4) {
+      const uint64_t blk = t >> 2;
+      const Philox4 o = philox4x32_10((uint32_t)blk, (uint32_t)(blk >> 32), i0, i1, k0, k1);
+      const uint32_t r[4] = {o.x, o.y, o.z, o.w};
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const uint32_t jj = sh == 32 ? 0u : (r[u] >> sh);
+        if (J.wide || (J.A >> 32)) {
+          const uint64_t v = J.A * (uint64_t)jj;
+          bump<kMode>(lane_base + (popc64(w ^ v) << 7));
+        } else {
+          bump<kMode>(lane_base + (__popc(wl ^ (a * jj)) << 7));
+        }
+      }
+    }
+    (void)wh;
+    for (; t < t1; ++t) {
+      const uint64_t v = J.A * mc_index(J.seed, i, t, J.n);
+      bump<kMode>(lane_base + (popc64(w ^ v) << 7));
+    }
+  } else {
+    for (uint64_t t = t0; t < t1; ++t) {
+      const uint64_t v = J.A * mc_index(J.seed, i, t, J.n);
+      bump<kMode>(lane_base + (popc64(w ^ v) << 7));
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Ext-Hamming weight tiles: 32 lanes x 256 generated messages.
+// ---------------------------------------------------------------------------
+template <int kMode>
+__device__ void weights_tile(const Job& J, uint64_t lt, uint32_t* wbins, int lane) {
+  const uint32_t lane_base = (uint32_t)__cvta_generic_to_shared(wbins) + (uint32_t)lane * 4u;
+  const uint64_t g0 = lt * (32ull * 256ull);
+#pragma unroll 4
+  for (uint32_t k = 0; k < 256; ++k) {
+    const uint64_t g = g0 + (uint64_t)k * 32 + lane;
+    if (g >= J.iters) break;
+    uint64_t x;
+    bool n4 = false;
+    if (J.wgen == WGEN_GRID) {
+      const uint64_t sh = g / J.shard, kk = g % J.shard;
+      const uint64_t wsh = sh * J.shard * (uint64_t)J.row_step;
+      x = (uint64_t)fma((double)kk, J.row_step, (double)wsh);
+    } else if (J.wgen == WGEN_MC) {
+      x = mc_index(J.seed, 0, g, J.bucket);
+    } else {
+      x = g;
+      n4 = true;
+    }
+    bump<kMode>(lane_base + (popc64(hamming_cw_gpu(x, J.bucket, n4)) << 7));
+  }
+}
+
+// ---------------------------------------------------------------------------
+// the persistent kernel
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t find_job(const Job* jobs, uint32_t njobs, uint64_t t) {
+  uint32_t lo = 0, hi = njobs - 1;
+  while (lo < hi) {
+    const uint32_t mid = (lo + hi + 1) >> 1;
+    if (__ldg(&jobs[mid].tile_begin) <= t) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+
+template <int kMode>
+__global__ void __launch_bounds__(kWarpsPerCta * 32) hist_kernel(LaunchArgs args) {
+  extern __shared__ __align__(16) uint32_t smem[];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const uint32_t per_warp = args.smem_bins * 32 + (args.use_col_table ? kTileCols : 0);
+  uint32_t* wbins = smem + warp * per_warp;
+  uint32_t* table = wbins + args.smem_bins * 32;
+  for (uint32_t k = lane; k < args.smem_bins * 32; k += 32) wbins[k] = 0;
+  __syncwarp();
+
+  uint32_t cur = 0xffffffffu;
+  uint32_t since_flush = 0;
+  Job J;
+  for (;;) {
+    unsigned long long t = 0;
+    if (lane == 0) t = atomicAdd(args.counter, 1ull);
+    t = __shfl_sync(0xffffffffu, t, 0);
+    if (t >= args.total_tiles) break;
+    const uint32_t jn = find_job(args.jobs, args.njobs, t);
+    if (jn != cur) {
+      if (cur != 0xffffffffu && since_flush) flush_bins(wbins, J.bins, J.nbins, lane);
+      since_flush = 0;
+      J = args.jobs[jn];
+      cur = jn;
+    }
+    const uint64_t lt = t - J.tile_begin;
+    if (J.kind == JOB_PAIRS) pairs_tile<kMode>(J, lt, wbins, table, lane);
+    else if (J.kind == JOB_MC) mc_tile<kMode>(J, lt, wbins, lane);
+    else weights_tile<kMode>(J, lt, wbins, lane);
+    if (++since_flush >= kFlushEvery) { flush_bins(wbins, J.bins, J.nbins, lane); since_flush = 0; }
+  }
+  if (cur != 0xffffffffu && since_flush) flush_bins(wbins, J.bins, J.nbins, lane);
+}
+
+// ---------------------------------------------------------------------------
+// POPC issue-rate probe: 8 independent popc chains per thread.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) popc_rate_kernel(uint32_t iters, uint32_t seed, uint32_t* sink) {
+  uint32_t x0 = seed ^ threadIdx.x, x1 = x0 * 3u + 1, x2 = x0 * 5u + 2, x3 = x0 * 7u + 3;
+  uint32_t x4 = x0 * 9u + 4, x5 = x0 * 11u + 5, x6 = x0 * 13u + 6, x7 = x0 * 15u + 7;
+  for (uint32_t i = 0; i < iters; ++i) {
+#pragma unroll
+    for (int u = 0; u < 16; ++u) {
+      x0 += __popc(x0); x1 += __popc(x1); x2 += __popc(x2); x3 += __popc(x3);
+      x4 += __popc(x4); x5 += __popc(x5); x6 += __popc(x6); x7 += __popc(x7);
+    }
+  }
+  const uint32_t r = x0 ^ x1 ^ x2 ^ x3 ^ x4 ^ x5 ^ x6 ^ x7;
+  if (r == 0x12345678u) sink[blockIdx.x] = r;
+}
+
+// ---------------------------------------------------------------------------
+// host-callable launchers
+// ---------------------------------------------------------------------------
+size_t hist_smem_bytes(uint32_t smem_bins, bool col_table) {
+  return (size_t)kWarpsPerCta * ((size_t)smem_bins * 32 + (col_table ? kTileCols : 0)) * sizeof(uint32_t);
+}
+
+static const void* kernel_ptr(int mode) {
+  return mode == HIST_RED ? (const void*)hist_kernel<HIST_RED> : (const void*)hist_kernel<HIST_LDST>;
+}
+
+cudaError_t hist_occupancy(int mode, size_t smem, int* ctas_per_sm) {
+  cudaError_t e = cudaFuncSetAttribute(kernel_ptr(mode), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  return cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas_per_sm, kernel_ptr(mode), kWarpsPerCta * 32, smem);
+}
+
+cudaError_t launch_hist(int mode, const LaunchArgs& args, int grid, size_t smem, cudaStream_t stream) {
+  cudaError_t e = cudaFuncSetAttribute(kernel_ptr(mode), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  if (mode == HIST_RED)
+    hist_kernel<HIST_RED><<<grid, kWarpsPerCta * 32, smem, stream>>>(args);
+  else
+    hist_kernel<HIST_LDST><<<grid, kWarpsPerCta * 32, smem, stream>>>(args);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_popc_rate(uint32_t iters, int grid, uint32_t* sink, cudaStream_t stream) {
+  popc_rate_kernel<<<grid, 256, 0, stream>>>(iters, 0x9e3779b9u, sink);
+  return cudaGetLastError();
+}
+
+}  // namespace dd

@@ -1,0 +1,194 @@
+/*
+ * codrel_b200.h — C-ABI of the B200-native distance-distribution library.
+ *
+ * The library computes Hamming-distance histograms over the codewords of
+ *   - AN codes:      cw(x) = A * x,            x in [0, 2^n)
+ *   - Ext. Hamming:  cw(x) = x | parity bits,  x in [0, 2^n)
+ * in exhaustive, 1-D/2-D grid and Monte Carlo modes, on one GPU.
+ *
+ * The reference tool (brics-db/coding_reliability, `distance_distribution`) has
+ * no plugin/FFI layer: its boundary is the set of C++ driver functions declared
+ * in distance_distribution/src/algorithms.h:20-34 and
+ * distance_distribution_super_a/src/algorithms.h:20-21.  Every such driver does
+ * (1) cudaMalloc + cudaMemset of <=64 uint64 bins, (2) one kernel launch per
+ * device, (3) a D2H copy and host sum, (4) a host post-processing step.  The
+ * entry points below replace steps (1)-(4) for one instance (dd_histogram), for
+ * a batch of instances in one persistent launch (dd_batch_run), and for a
+ * stream of queries (dd_server_*).  The C++ shims with the reference's own
+ * names and signatures (codrel_dropin.h) sit on top of these.
+ *
+ * Conventions (all functions):
+ *   - plain C types, caller-owned host buffers, no exit(): every call returns
+ *     a dd_status; dd_last_error() gives a one-line message for the calling
+ *     thread's last failure.  (The reference prints and exit()s through
+ *     CHECK_ERROR, distance_distribution/lib/helper/inc/globals_cuda.h:42-74,
+ *     and throws std::runtime_error for an unsupported n or bin count,
+ *     src/an_coding.h:56, src/an_coding.cu:165.)
+ *   - a dd_context owns one device, one CUDA stream and its device state; one
+ *     context must not be used by two host threads at the same time, distinct
+ *     contexts may.
+ *   - uint128 counts are returned as (lo, hi) uint64 pairs.
+ */
+#ifndef CODREL_B200_H_
+#define CODREL_B200_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DD_MAX_BINS 64   /* COUNTS_MAX_WIDTH, distance_distribution_super_a/src/globals.h:44 */
+#define DD_ABI_VERSION 1
+
+typedef enum dd_status {
+  DD_OK = 0,
+  DD_ERR_INVALID_ARGUMENT = 1, /* malformed request (reference: assert / runtime_error) */
+  DD_ERR_UNSUPPORTED = 2,      /* n or bin count outside what the kernels handle */
+  DD_ERR_CUDA = 3,             /* a CUDA runtime call failed (reference: CHECK_ERROR -> exit) */
+  DD_ERR_NO_DEVICE = 4,        /* no CUDA device / CUDA library not usable */
+  DD_ERR_OUT_OF_MEMORY = 5,    /* device allocation failed or memory budget exceeded */
+  DD_ERR_BUSY = 6,             /* server: admission refused (queue full) */
+  DD_ERR_TIMEOUT = 7,          /* a bounded device-side wait ran out */
+  DD_ERR_NOT_FOUND = 8,        /* server: unknown ticket */
+  DD_ERR_CANCELLED = 9         /* server shut down before the query ran */
+} dd_status;
+
+typedef enum dd_code { DD_CODE_AN = 0, DD_CODE_EXT_HAMMING = 1 } dd_code;
+
+typedef enum dd_mode {
+  DD_MODE_EXHAUSTIVE = 0,  /* all pairs */
+  DD_MODE_GRID_1D = 1,     /* codewords x lattice of m points (an_coding_grid.cu:60-114) */
+  DD_MODE_GRID_2D = 2,     /* lattice of m2 points x lattice of m points (an_coding_grid.cu:121-140) */
+  DD_MODE_MONTE_CARLO = 3  /* Philox4x32-10 sampled pairs (replaces cuRAND Sobol32) */
+} dd_mode;
+
+/* Which kernel family computes an AN exhaustive histogram. */
+typedef enum dd_kernel {
+  DD_KERNEL_AUTO = 0,  /* autotuner's choice for the shape */
+  DD_KERNEL_POPC = 1,  /* XOR + POPC, warp-private shared-memory bins */
+  DD_KERNEL_MMA = 2    /* tcgen05 kind::i8 bit-plane MMA, histogram epilogue from TMEM */
+} dd_kernel;
+
+/* Ext-Hamming exhaustive algorithm (reference `-e` switch, src/main.cpp:245-268). */
+typedef enum dd_hamming_method {
+  DD_HAMMING_WEIGHTS = 0,   /* `-e 1`: weight enumerator x 2^n (src/hamming.cu:64-224) */
+  DD_HAMMING_ALL_PAIRS = 1,  /* `-e 2` / `-e 4`: every ordered codeword pair incl. a==b
+                                (+ the 1-bit spheres of the second codeword),
+                                src/hamming_native_short.cpp:29-84, src/hamming_native.cpp:39-113 */
+  DD_HAMMING_ALL_PAIRS_DISTINCT = 2  /* `-e 3`: pairs a<b (+ spheres of b), doubled; no a==b term,
+                                        src/hamming_native_short_ordering.cpp:39-84 */
+} dd_hamming_method;
+
+/* Which reference driver's host conventions a request follows. */
+typedef enum dd_convention {
+  DD_CONV_GPU = 0,     /* run_ancoding & co (src/an_coding.cu:276-280): power-of-two A -> 1,
+                          h = ceil(log(A)/log(2)), minb searched in [1, nbins/2) */
+  DD_CONV_CPU = 1,     /* run_ancoding_cpu (src/an_coding.cpp:104-142): A kept as given */
+  DD_CONV_SUPER_A = 2  /* super-A fork (super_a/src/an_coding.cu:135-244): h given by the caller
+                          (floor(log(A)/log(2))+1), minb searched in [1, (nbins+1)/2) */
+} dd_convention;
+
+typedef struct dd_request {
+  uint32_t code;            /* dd_code */
+  uint32_t mode;            /* dd_mode */
+  uint64_t A;               /* AN multiplier (ignored for Hamming); 0 is read as 1 (src/main.cpp:79) */
+  uint32_t n;               /* data bits k */
+  uint32_t h;               /* 0: derive as `convention` says; else the check-bit count to use */
+  uint64_t m;               /* grid points (1st dim) / Monte Carlo iterations */
+  uint64_t m2;              /* 2-D grid: points of the 2nd dim (0 -> m, src/main.cpp:127-128) */
+  uint64_t seed;            /* Monte Carlo: Philox key */
+  uint32_t with_1bit;       /* Ext-Hamming: add the 1-bit spheres (`-b`) */
+  uint32_t hamming_method;  /* dd_hamming_method */
+  uint32_t kernel;          /* dd_kernel */
+  uint32_t convention;      /* dd_convention */
+  uint64_t user_tag;        /* opaque, copied to the result */
+} dd_request;
+
+typedef struct dd_result {
+  uint32_t status;          /* dd_status of this instance */
+  uint32_t nbins;           /* n + h + 1 */
+  uint32_t h;               /* check bits used */
+  uint32_t kernel_used;     /* dd_kernel that ran */
+  uint64_t A;               /* A after the convention's normalisation */
+  uint64_t iterations;      /* m after capping at 2^n (grid / MC), else 0 */
+  uint64_t iterations2;     /* m2 after capping (2-D grid), else 0 */
+  uint64_t pairs_lo, pairs_hi;  /* distance evaluations the device performed (uint128) */
+  uint64_t raw[DD_MAX_BINS];    /* device histogram: the reference's host-summed hcounts[0][] */
+  uint64_t counts_lo[DD_MAX_BINS];  /* post-processed uint128 counts[] (lo 64 bits) */
+  uint64_t counts_hi[DD_MAX_BINS];  /*                                  (hi 64 bits) */
+  uint64_t minb;            /* first non-zero bin in the convention's range, 0xFFFF if none */
+  uint64_t mincb_lo, mincb_hi;
+  double max_rel_error;     /* get_rel_error_AN / get_abs_error_hamming as the driver returns it,
+                               -1 when the reference has no golden table for (A, n) */
+  double kernel_ms;         /* device time of the histogram kernel(s), CUDA events */
+  double total_ms;          /* host wall time of the whole call */
+  uint64_t user_tag;
+} dd_result;
+
+typedef struct dd_context dd_context;
+
+/* --- library ---------------------------------------------------------- */
+const char* dd_version(void);
+const char* dd_status_string(int status);
+/* Message of the calling thread's last failed call ("" if none). */
+const char* dd_last_error(void);
+/* Number of CUDA devices (0 when none / no driver). Never fails. */
+int dd_device_count(void);
+
+/* --- contexts ----------------------------------------------------------- */
+/* device: CUDA ordinal.  stream: a cudaStream_t to issue all work on, or NULL
+ * for a stream the context creates and owns. */
+int dd_context_create(int device, void* stream, dd_context** out);
+int dd_context_destroy(dd_context* ctx);
+
+/* --- one instance ------------------------------------------------------- */
+/* Computes one histogram synchronously: launch on the context's stream,
+ * D2H of the raw bins, host post-processing.  Replaces run_ancoding,
+ * run_ancoding_grid, run_ancoding_mc (src/an_coding*.cu), run_hamming,
+ * run_hamming_grid, run_hamming_mc (src/hamming*.cu), run_ancoding_cpu
+ * (src/an_coding.cpp:104), run_hamming_cpu* (src/hamming*.cpp) and the
+ * super-A run_ancoding (super_a/src/an_coding.cu:135). */
+int dd_histogram(dd_context* ctx, const dd_request* req, dd_result* res);
+
+/* --- batch -------------------------------------------------------------- */
+typedef struct dd_batch_options {
+  uint32_t use_graph;       /* capture the launch in a CUDA graph and replay it */
+  uint32_t kernel;          /* dd_kernel for every AN exhaustive instance (AUTO: autotuner) */
+  uint32_t ctas_per_sm;     /* 0: autotuner */
+  uint32_t reserved;
+} dd_batch_options;
+
+/* Runs `count` AN exhaustive instances (any mix of A and n) in ONE persistent
+ * launch.  Replaces the super-A sweeps' sequential run_ancoding calls
+ * (src/main.cpp:131-177, super_a/src/main.cpp:194-297).  Non-exhaustive or
+ * Hamming requests in the batch are run one after the other on the stream. */
+int dd_batch_run(dd_context* ctx, const dd_request* reqs, uint32_t count,
+                 dd_result* results, const dd_batch_options* opts);
+
+/* --- host-only helpers (no device needed) ------------------------------- */
+/* Derives nbins/h/A for a request exactly as the reference's drivers do. */
+int dd_request_shape(const dd_request* req, uint32_t* nbins, uint32_t* h, uint64_t* A_eff);
+/* The reference's post-processing of a raw device histogram into counts[],
+ * minb/mincb and the error estimate (the host tail of every run_* driver). */
+int dd_postprocess(const dd_request* req, const uint64_t* raw, uint32_t nraw, dd_result* res);
+/* Renders a result in the reference's results-file layout
+ * (process_result, src/globals.cpp:185-305): writes at most cap bytes
+ * (NUL-terminated) and stores the full length in *len.  `device_line` is
+ * appended as the reference appends its "Device" lines (may be NULL). */
+int dd_format_result(const dd_request* req, const dd_result* res, const char* device_line,
+                     char* buf, size_t cap, size_t* len);
+/* Philox4x32-10 (Salmon et al., SC'11), the counter-based generator behind
+ * Monte Carlo mode: out = philox(ctr, key). */
+void dd_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);
+
+/* --- measurement -------------------------------------------------------- */
+/* Measures the device's POPC issue rate (popc/s) with a dependency-free POPC
+ * loop on the context's stream. */
+int dd_measure_popc_peak(dd_context* ctx, double* popc_per_s);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CODREL_B200_H_ */

@@ -1,0 +1,254 @@
+"""Parity of the GPU path (through the C-ABI) with the oracle and the
+reference's golden data.  Bit-exact for every histogram: the arithmetic is
+integer, and the grid lattice's double arithmetic is the reference's own."""
+import random
+
+import pytest
+
+import coding_reliability_b200 as dd
+import oracle
+from conftest import golden
+
+pytestmark = pytest.mark.gpu
+
+
+def an_req(A, n, **kw):
+    return dd.Request(dd.CODE_AN, dd.MODE_EXHAUSTIVE, A, n, **kw)
+
+
+# -- AN exhaustive --------------------------------------------------------------
+@pytest.mark.parametrize("A", [1, 3, 61, 255, 641, 1021, 32771, 58659, 65521])
+@pytest.mark.parametrize("n", [1, 2, 3, 5, 7, 9, 10, 11, 12])
+def test_an_exhaustive_small(ctx, A, n):
+    req = an_req(A, n)
+    nb, h, Aeff = dd.request_shape(req)
+    res = ctx.histogram(req)
+    assert res.raw == oracle.an_exhaustive_raw(Aeff, n, nb)
+    assert res.counts == oracle.an_exhaustive_counts(Aeff, n, nb)
+    assert sum(res.raw) == (1 << n) * ((1 << n) - 1) // 2
+
+
+@pytest.mark.parametrize("A,n", [(61, 8), (641, 8), (61, 16), (641, 16)])
+def test_an_solutions_h(ctx, A, n):
+    sol = golden("solutions.json")[f"solution_an{n}_A{A}"]
+    res = ctx.histogram(an_req(A, n))
+    k = min(len(sol), res.nbins)
+    assert res.counts[:k] == sol[:k]
+
+
+def test_an_results_archive(ctx):
+    """results/As exhaustive histograms n=8..22 (every A of the archive)."""
+    cases = [c for c in golden("an_exhaustive.json") if c["n"] <= 22]
+    assert len(cases) > 600
+    for c in cases:
+        res = ctx.histogram(an_req(c["A"], c["n"]))
+        assert res.h == c["h"], c["file"]
+        assert res.counts == c["counts"], c["file"]
+
+
+@pytest.mark.parametrize("A,n", [(58659, 13), (58659, 16), (65521, 16), (641, 18), (3, 20)])
+def test_an_wide_and_mid(ctx, A, n):
+    """40-bit style codewords (n+h > 32 for n>=17 at 16-bit A) and mid sizes vs the oracle."""
+    req = an_req(A, n)
+    nb, h, Aeff = dd.request_shape(req)
+    res = ctx.histogram(req)
+    assert res.raw == oracle.an_exhaustive_raw(Aeff, n, nb)
+
+
+@pytest.mark.parametrize("A,n", [(58659, 18), (32771, 17), (65535, 17)])
+def test_an_wide_codewords(ctx, A, n):
+    """Codewords above 32 bits: the high-word segment split of the popc kernel."""
+    req = an_req(A, n)
+    nb, h, Aeff = dd.request_shape(req)
+    assert (Aeff * ((1 << n) - 1)) >> 32
+    res = ctx.histogram(req)
+    assert res.raw == oracle.an_exhaustive_raw(Aeff, n, nb)
+
+
+@pytest.mark.parametrize("conv", [dd.CONV_GPU, dd.CONV_CPU, dd.CONV_SUPER_A])
+def test_an_conventions(ctx, conv):
+    for A in (64, 58659, 641):
+        req = an_req(A, 12, convention=conv)
+        nb, h, Aeff = dd.request_shape(req)
+        res = ctx.histogram(req)
+        assert res.counts == oracle.an_exhaustive_counts(Aeff, 12, nb)
+        lim = (nb + 1) // 2 if conv == dd.CONV_SUPER_A else nb // 2
+        first = next((i for i in range(1, lim) if res.counts[i]), 0xFFFF)
+        assert res.minb == first
+
+
+def test_an_k24_archive_A63877(ctx):
+    """The config-3 shape (16-bit A, k=24, 41 bins) against the reference's archived exhaustive run."""
+    case = next(c for c in golden("an_exhaustive.json") if c["A"] == 63877 and c["n"] == 24)
+    res = ctx.histogram(an_req(63877, 24))
+    assert res.counts == case["counts"]
+
+
+def test_an_k24_solutions_A641(ctx):
+    sol = golden("solutions.json")["solution_an24_A641"]
+    res = ctx.histogram(an_req(641, 24))
+    assert res.counts == sol[: res.nbins]
+
+
+# -- AN grid ---------------------------------------------------------------------
+def test_an_grid1d_archive(ctx):
+    """Every archived 1-D grid run with n <= 24 (m up to 10^6, non-power-of-two steps)."""
+    checked = 0
+    for x in golden("an_grid1d.json"):
+        if x["n"] > 24 or any(isinstance(c, str) for c in x["counts"]):
+            continue
+        res = ctx.histogram(dd.Request(dd.CODE_AN, dd.MODE_GRID_1D, x["A"], x["n"], m=x["m"]))
+        assert res.counts == x["counts"], x["file"]
+        checked += 1
+    assert checked >= 90
+
+
+@pytest.mark.parametrize("A,n,m", [(61, 12, 3), (61, 12, 16), (61, 12, 17), (641, 14, 1000), (58659, 16, 4096),
+                                   (58659, 18, 77), (3, 10, 1024), (65521, 17, 333)])
+def test_an_grid1d_oracle(ctx, A, n, m):
+    req = dd.Request(dd.CODE_AN, dd.MODE_GRID_1D, A, n, m=m)
+    nb, h, Aeff = dd.request_shape(req)
+    res = ctx.histogram(req)
+    raw, _ = oracle.an_grid1d_raw(Aeff, n, h, m, nb)
+    assert res.raw == raw
+
+
+@pytest.mark.parametrize("A,n,m,m2", [(61, 12, 100, 37), (641, 14, 64, 64), (58659, 18, 50, 300), (3, 8, 256, 1)])
+def test_an_grid2d_oracle(ctx, A, n, m, m2):
+    req = dd.Request(dd.CODE_AN, dd.MODE_GRID_2D, A, n, m=m, m2=m2)
+    nb, h, Aeff = dd.request_shape(req)
+    res = ctx.histogram(req)
+    raw = oracle.an_grid2d_raw(Aeff, n, m, m2, nb)
+    assert res.raw[1:] == raw[1:] and res.raw[0] == 0
+    assert res.counts == oracle.an_grid_counts(2, n, min(m, 1 << n), min(m2, 1 << n), raw)
+
+
+# -- AN Monte Carlo ----------------------------------------------------------------
+@pytest.mark.parametrize("A,n,it,seed", [(61, 10, 100, 1), (641, 12, 257, 99), (58659, 16, 13, 7),
+                                         (58659, 18, 4, 2026), (61, 33, 1, 5)])
+def test_an_mc_replay(ctx, A, n, it, seed):
+    """Exact equality with the CPU replay of the same Philox counter stream."""
+    req = dd.Request(dd.CODE_AN, dd.MODE_MONTE_CARLO, A, n, m=it, seed=seed)
+    nb, h, Aeff = dd.request_shape(req)
+    if n > 24:
+        pytest.skip("n=33 replay is too long on the CPU")
+    res = ctx.histogram(req)
+    assert res.raw == oracle.an_mc_raw(Aeff, n, it, seed, nb)
+    assert res.counts == oracle.an_mc_counts(n, min(it, 1 << n), res.raw)
+
+
+def test_an_mc_statistical_agreement(ctx):
+    """MC estimate vs the exact solutions.h histogram (A=61, n=16): every well-populated
+    bin within 5 standard deviations of its binomial sampling noise."""
+    sol = golden("solutions.json")["solution_an16_A61"]
+    it = 4096
+    res = ctx.histogram(dd.Request(dd.CODE_AN, dd.MODE_MONTE_CARLO, 61, 16, m=it, seed=12345))
+    N = 1 << 16
+    total = N * it
+    for d in range(1, res.nbins):
+        p = sol[d] / (N * N)
+        if p * total < 1000:
+            continue
+        sd = (total * p * (1 - p)) ** 0.5
+        assert abs(res.raw[d] - total * p) < 5 * sd, d
+
+
+# -- Ext-Hamming ------------------------------------------------------------------
+@pytest.mark.parametrize("n", [4, 8, 16, 24, 32])
+@pytest.mark.parametrize("w1", [0, 1])
+def test_hamming_weights(ctx, n, w1):
+    req = dd.Request(dd.CODE_EXT_HAMMING, dd.MODE_EXHAUSTIVE, 1, n, with_1bit=w1)
+    nb, h, _ = dd.request_shape(req)
+    res = ctx.histogram(req)
+    if n <= 24:
+        assert res.raw == oracle.hamming_weights_raw(n, nb)
+    assert res.counts == oracle.hamming_weights_counts(n, w1, res.raw)
+    if n in (8, 16, 24, 32):
+        sol = golden("solutions.json")[f"sol_hamming_n{n}"]
+        for i in range(4, nb, 2):
+            assert res.counts[i] == sol[i] << n
+
+
+@pytest.mark.parametrize("run", [r for r in golden("ref_runs.json") if r["args"][0] == "-e"],
+                         ids=lambda r: " ".join(r["args"]))
+def test_hamming_reference_runs(ctx, run):
+    args = run["args"]
+    n = int(args[-1])
+    method = {"1": dd.HAMMING_WEIGHTS, "2": dd.HAMMING_ALL_PAIRS, "3": dd.HAMMING_ALL_PAIRS_DISTINCT,
+              "4": dd.HAMMING_ALL_PAIRS}[args[1]]
+    res = ctx.histogram(dd.Request(dd.CODE_EXT_HAMMING, dd.MODE_EXHAUSTIVE, 1, n, with_1bit=int("-b" in args),
+                                   hamming_method=method))
+    assert res.counts == run["counts"]
+
+
+@pytest.mark.parametrize("n", [8, 16, 24])
+def test_hamming_all_pairs_vs_weights(ctx, n):
+    """All-pairs brute force (2^2n pairs on the GPU) equals the weight enumerator, with spheres."""
+    for w1 in (0, 1):
+        a = ctx.histogram(dd.Request(dd.CODE_EXT_HAMMING, dd.MODE_EXHAUSTIVE, 1, n, with_1bit=w1,
+                                     hamming_method=dd.HAMMING_ALL_PAIRS))
+        b = ctx.histogram(dd.Request(dd.CODE_EXT_HAMMING, dd.MODE_EXHAUSTIVE, 1, n, with_1bit=w1))
+        assert a.counts == b.counts
+        if n == 8:
+            assert a.counts == oracle.hamming_pairs_raw(8, w1, a.nbins)
+
+
+@pytest.mark.parametrize("n,m", [(8, 100), (16, 1000), (16, 4096), (24, 99999), (32, 1 << 20)])
+def test_hamming_grid(ctx, n, m):
+    for w1 in (0, 1):
+        req = dd.Request(dd.CODE_EXT_HAMMING, dd.MODE_GRID_1D, 1, n, m=m, with_1bit=w1)
+        nb, h, _ = dd.request_shape(req)
+        res = ctx.histogram(req)
+        raw, _ = oracle.hamming_grid_raw(n, m, nb)
+        assert res.raw == raw
+        assert res.counts == oracle.hamming_sampled_counts(0, n, w1, min(m, 1 << n), raw)
+
+
+@pytest.mark.parametrize("n,m,seed", [(8, 100, 1), (16, 5000, 2), (24, 1 << 16, 3), (40, 1 << 16, 4)])
+def test_hamming_mc(ctx, n, m, seed):
+    req = dd.Request(dd.CODE_EXT_HAMMING, dd.MODE_MONTE_CARLO, 1, n, m=m, seed=seed, with_1bit=1)
+    nb, h, _ = dd.request_shape(req)
+    res = ctx.histogram(req)
+    raw, _ = oracle.hamming_mc_raw(n, m, seed, nb)
+    assert res.raw == raw
+    assert res.counts == oracle.hamming_sampled_counts(1, n, 1, min(m, 1 << n), raw)
+
+
+# -- batch ---------------------------------------------------------------------------
+def super_a_set(count=256, seed=20261203):
+    rng = random.Random(seed)
+    out = []
+    while len(out) < count:
+        a = rng.randrange(32768, 65536) | 1
+        if a not in out:
+            out.append(a)
+    return out
+
+
+def test_batch_equals_single(ctx):
+    reqs = [an_req(A, 12, convention=dd.CONV_SUPER_A) for A in super_a_set(64)]
+    reqs += [an_req(641, 12), an_req(61, 9), dd.Request(dd.CODE_AN, dd.MODE_GRID_1D, 61, 14, m=333),
+             dd.Request(dd.CODE_AN, dd.MODE_MONTE_CARLO, 58659, 12, m=50, seed=3),
+             dd.Request(dd.CODE_EXT_HAMMING, dd.MODE_EXHAUSTIVE, 1, 16, with_1bit=1)]
+    for graph in (False, True, True):
+        out = ctx.batch(reqs, use_graph=graph)
+        for q, r in zip(reqs, out):
+            s = ctx.histogram(q)
+            assert r.counts == s.counts and r.raw == s.raw and r.minb == s.minb
+
+
+def test_super_a_sweep_k16_batched(ctx):
+    """The 256-candidate k=16 sweep in one launch: every instance equals its own run,
+    and the archived sweep pins (results/superAs/superA_n16_h16.txt) hold."""
+    As = super_a_set(256)
+    reqs = [an_req(A, 16, convention=dd.CONV_SUPER_A) for A in As]
+    out = ctx.batch(reqs, use_graph=True)
+    for A, r in list(zip(As, out))[::32]:
+        s = ctx.histogram(an_req(A, 16, convention=dd.CONV_SUPER_A))
+        assert r.counts == s.counts
+    pins = next(f for f in golden("super_a.json") if f["n"] == 16 and f["h"] == 16)["pins"]
+    pin_reqs = [an_req(A, 16) for A, _, _ in pins]
+    for (A, minb, mincb), r in zip(pins, ctx.batch(pin_reqs)):
+        assert (r.minb, r.mincb) == (minb, mincb), A
+    # one exact oracle check of the batch
+    assert out[0].raw == oracle.an_exhaustive_raw(As[0], 16, out[0].nbins)

@@ -21,7 +21,7 @@ __all__ = [
     "CODE_AN", "CODE_EXT_HAMMING", "MODE_EXHAUSTIVE", "MODE_GRID_1D", "MODE_GRID_2D", "MODE_MONTE_CARLO",
     "KERNEL_AUTO", "KERNEL_POPC", "KERNEL_MMA", "HAMMING_WEIGHTS", "HAMMING_ALL_PAIRS", "HAMMING_ALL_PAIRS_DISTINCT",
     "CONV_GPU", "CONV_CPU", "CONV_SUPER_A", "MAX_BINS", "DDError", "Request", "Result", "Context",
-    "load", "lib_path", "postprocess", "format_result", "request_shape", "philox4x32_10", "device_count",
+    "load", "lib_path", "postprocess", "request_plan", "format_result", "request_shape", "philox4x32_10", "device_count",
     "run_ancoding", "run_ancoding_cpu", "run_ancoding_grid", "run_ancoding_mc", "run_hamming",
     "run_hamming_grid", "run_hamming_mc",
 ]
@@ -148,6 +148,8 @@ def load() -> C.CDLL:
     lib.dd_batch_run.argtypes = [vp, C.POINTER(_Req), u32, C.POINTER(_Res), C.POINTER(_BatchOpts)]
     lib.dd_request_shape.argtypes = [C.POINTER(_Req), C.POINTER(u32), C.POINTER(u32), C.POINTER(C.c_uint64)]
     lib.dd_postprocess.argtypes = [C.POINTER(_Req), C.POINTER(C.c_uint64), u32, C.POINTER(_Res)]
+    u64p = C.POINTER(C.c_uint64)
+    lib.dd_request_plan.argtypes = [C.POINTER(_Req), u64p, u64p, u64p, u64p]
     lib.dd_format_result.argtypes = [C.POINTER(_Req), C.POINTER(_Res), C.c_char_p, C.c_char_p, C.c_size_t,
                                      C.POINTER(C.c_size_t)]
     lib.dd_philox4x32_10.argtypes = [C.POINTER(u32), C.POINTER(u32), C.POINTER(u32)]
@@ -170,6 +172,13 @@ def request_shape(req: Request) -> tuple[int, int, int]:
     nb, h, a = C.c_uint32(), C.c_uint32(), C.c_uint64()
     _check(load().dd_request_shape(C.byref(req._c()), C.byref(nb), C.byref(h), C.byref(a)))
     return nb.value, h.value, a.value
+
+
+def request_plan(req: Request) -> dict:
+    """Device work a request plans (no device needed): lattice points, tiles, pairs."""
+    lat, tiles, lo, hi = C.c_uint64(), C.c_uint64(), C.c_uint64(), C.c_uint64()
+    _check(load().dd_request_plan(C.byref(req._c()), C.byref(lat), C.byref(tiles), C.byref(lo), C.byref(hi)))
+    return {"lattice": lat.value, "tiles": tiles.value, "pairs": (hi.value << 64) | lo.value}
 
 
 def postprocess(req: Request, raw: list[int]) -> Result:

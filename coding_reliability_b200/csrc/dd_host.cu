@@ -20,6 +20,7 @@
 #include "dd_device.cuh"
 #include "dd_host.h"
 #include "dd_kernels.h"
+#include "dd_mma.h"
 
 struct dd_context {
   int device = 0;
@@ -29,25 +30,28 @@ struct dd_context {
   // device state
   unsigned long long* d_bins = nullptr;  // bin_slots x kMaxBins
   uint32_t bin_slots = 0;
-  unsigned long long* d_counter = nullptr;
+  unsigned long long* d_ctl = nullptr;   // [0] popc work counter, [1] MMA work counter, [2] status, [3..15] diagnostics
   dd::Job* d_jobs = nullptr;
   uint32_t job_cap = 0;
   // pinned host mirrors
   unsigned long long* h_bins = nullptr;
+  unsigned long long* h_ctl = nullptr;
   dd::Job* h_jobs = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   // tuning
   int hist_mode = dd::HIST_RED;
   int tuned = 0;
+  unsigned long long mma_timeout_ns = 2000000000ull;  // bound of every device-side wait
   // batch graph cache
   cudaGraphExec_t gexec = nullptr;
   std::vector<dd::Job> gjobs;  // job table the cached graph was built for
-  int ggrid = 0;
-  size_t gsmem = 0;
+  int ggrid[2] = {0, 0};
+  size_t gsmem[2] = {0, 0};
 };
 
 namespace dd {
 
+constexpr int kCtlWords = 16;
 static thread_local std::string t_last_error;
 void set_error(const std::string& msg) { t_last_error = msg; }
 
@@ -92,52 +96,123 @@ static int ensure_capacity(dd_context* ctx, uint32_t slots, uint32_t njobs) {
 }
 
 struct LaunchPlan {
-  LaunchArgs args;
-  int grid = 0;
-  size_t smem = 0;
+  LaunchArgs pargs;          // popc kernel: table entries [0, npopc)
+  int pgrid = 0;
+  size_t psmem = 0;
+  uint32_t npopc = 0;
+  MmaArgs margs;             // MMA kernel: table entries [npopc, npopc + nmma)
+  int mgrid = 0;
+  size_t msmem = 0;
+  uint32_t nmma = 0;
+  uint32_t nslots = 0;       // bin slots (one per request, in request order)
 };
 
-// Fills the pinned job table, assigns tile ranges and bin slots, and sizes
-// the persistent grid (one wave: SMs x resident CTAs).
-static int plan_launch(dd_context* ctx, std::vector<Job>& jobs, LaunchPlan& lp) {
-  uint64_t t = 0;
-  uint32_t maxb = 1;
-  bool table = false;
-  for (size_t i = 0; i < jobs.size(); ++i) {
-    jobs[i].tile_begin = t;
-    t += jobs[i].tiles;
-    jobs[i].bins = ctx->d_bins + i * kMaxBins;
-    maxb = std::max(maxb, jobs[i].nbins);
-    table |= (jobs[i].kind == JOB_PAIRS && jobs[i].col_kind == COL_HAMMING_EXT && !jobs[i].wide);
+// Which kernel runs a job: explicit MMA or POPC requests are honoured where
+// the job allows them; AUTO uses the context's measured preference.
+static bool want_mma(const dd_context* ctx, const Job& j, uint32_t kernel) {
+  if (!mma_eligible(j)) return false;
+  if (kernel == DD_KERNEL_MMA) return true;
+  if (kernel == DD_KERNEL_POPC) return false;
+  return ctx->tuned == 2;  // autotuner's verdict for AN exhaustive shapes
+}
+
+// Orders the job table (popc jobs first, then MMA jobs), assigns tile ranges
+// and bin slots (slot = request index), and sizes both persistent grids.
+static int plan_launch(dd_context* ctx, std::vector<Job>& jobs, const std::vector<uint32_t>& kernels,
+                       LaunchPlan& lp) {
+  std::vector<Job> table;
+  table.reserve(jobs.size());
+  for (int pass = 0; pass < 2; ++pass)
+    for (size_t i = 0; i < jobs.size(); ++i) {
+      const bool m = want_mma(ctx, jobs[i], kernels[i]);
+      if ((pass == 1) != m) continue;
+      Job j = jobs[i];
+      j.bins = ctx->d_bins + i * kMaxBins;
+      table.push_back(j);
+    }
+  lp.nslots = (uint32_t)jobs.size();
+  uint64_t tp = 0, tm = 0;
+  uint32_t maxb = 1, maxbm = 1;
+  bool col_table = false;
+  lp.npopc = 0;
+  for (size_t i = 0; i < jobs.size(); ++i) lp.npopc += want_mma(ctx, jobs[i], kernels[i]) ? 0 : 1;
+  lp.nmma = (uint32_t)table.size() - lp.npopc;
+  for (uint32_t k = 0; k < lp.npopc; ++k) {
+    Job& j = table[k];
+    j.tile_begin = tp;
+    tp += j.tiles;
+    maxb = std::max(maxb, j.nbins);
+    col_table |= (j.kind == JOB_PAIRS && j.col_kind == COL_HAMMING_EXT && !j.wide);
   }
-  lp.args.jobs = ctx->d_jobs;
-  lp.args.njobs = (uint32_t)jobs.size();
-  lp.args.smem_bins = maxb;
-  lp.args.total_tiles = t;
-  lp.args.counter = ctx->d_counter;
-  lp.args.use_col_table = table ? 1u : 0u;
-  lp.smem = hist_smem_bytes(maxb, table);
-  int occ = 0;
-  DD_CUDA(hist_occupancy(ctx->hist_mode, lp.smem, &occ));
-  if (occ < 1) { set_error("kernel does not fit on an SM"); return DD_ERR_UNSUPPORTED; }
-  // never more warps than tiles
-  const uint64_t want = (t + kWarpsPerCta - 1) / kWarpsPerCta;
-  lp.grid = (int)std::min<uint64_t>((uint64_t)ctx->num_sms * occ, std::max<uint64_t>(want, 1));
-  std::memcpy(ctx->h_jobs, jobs.data(), jobs.size() * sizeof(Job));
+  for (uint32_t k = lp.npopc; k < table.size(); ++k) {
+    Job& j = table[k];
+    j.tile_begin = tm;
+    tm += j.tiles;
+    maxbm = std::max(maxbm, j.nbins);
+  }
+  unsigned* status = reinterpret_cast<unsigned*>(ctx->d_ctl + 2);
+  lp.pargs.jobs = ctx->d_jobs;
+  lp.pargs.njobs = lp.npopc;
+  lp.pargs.smem_bins = maxb;
+  lp.pargs.total_tiles = tp;
+  lp.pargs.counter = ctx->d_ctl;
+  lp.pargs.status = status;
+  lp.pargs.use_col_table = col_table ? 1u : 0u;
+  lp.pargs.pad = 0;
+  if (lp.npopc && tp) {
+    lp.psmem = hist_smem_bytes(maxb, col_table);
+    int occ = 0;
+    DD_CUDA(hist_occupancy(ctx->hist_mode, lp.psmem, &occ));
+    if (occ < 1) { set_error("kernel does not fit on an SM"); return DD_ERR_UNSUPPORTED; }
+    const uint64_t want = (tp + kWarpsPerCta - 1) / kWarpsPerCta;
+    lp.pgrid = (int)std::min<uint64_t>((uint64_t)ctx->num_sms * occ, std::max<uint64_t>(want, 1));
+  }
+  lp.margs.jobs = ctx->d_jobs + lp.npopc;
+  lp.margs.njobs = lp.nmma;
+  lp.margs.hist_rows = maxbm + 1;  // + the row that catches out-of-range distances
+  lp.margs.total_tiles = tm;
+  lp.margs.counter = ctx->d_ctl + 1;
+  lp.margs.status = status;
+  lp.margs.timeout_ns = ctx->mma_timeout_ns;
+  if (lp.nmma && tm) {
+    lp.msmem = mma_smem_bytes(lp.margs.hist_rows);
+    lp.mgrid = (int)std::min<uint64_t>((uint64_t)ctx->num_sms, tm);  // one CTA (one TMEM owner) per SM
+  }
+  std::memcpy(ctx->h_jobs, table.data(), table.size() * sizeof(Job));
   return DD_OK;
 }
 
-// Enqueues: job table H2D, bins + counter reset, kernel (bracketed by events), bins D2H.
-static int enqueue_launch(dd_context* ctx, const LaunchPlan& lp, uint32_t njobs, bool events) {
+// Enqueues: job table H2D, bins / counters / status reset, kernels (bracketed
+// by events), bins + status D2H.
+static int enqueue_launch(dd_context* ctx, const LaunchPlan& lp) {
   cudaStream_t s = ctx->stream;
+  const uint32_t njobs = lp.npopc + lp.nmma;
   DD_CUDA(cudaMemcpyAsync(ctx->d_jobs, ctx->h_jobs, njobs * sizeof(Job), cudaMemcpyHostToDevice, s));
-  DD_CUDA(cudaMemsetAsync(ctx->d_bins, 0, (size_t)njobs * kMaxBins * sizeof(unsigned long long), s));
-  DD_CUDA(cudaMemsetAsync(ctx->d_counter, 0, sizeof(unsigned long long), s));
-  if (events) DD_CUDA(cudaEventRecord(ctx->ev0, s));
-  if (lp.args.total_tiles) DD_CUDA(launch_hist(ctx->hist_mode, lp.args, lp.grid, lp.smem, s));
-  if (events) DD_CUDA(cudaEventRecord(ctx->ev1, s));
-  DD_CUDA(cudaMemcpyAsync(ctx->h_bins, ctx->d_bins, (size_t)njobs * kMaxBins * sizeof(unsigned long long),
+  DD_CUDA(cudaMemsetAsync(ctx->d_bins, 0, (size_t)lp.nslots * kMaxBins * sizeof(unsigned long long), s));
+  DD_CUDA(cudaMemsetAsync(ctx->d_ctl, 0, kCtlWords * sizeof(unsigned long long), s));
+  DD_CUDA(cudaEventRecord(ctx->ev0, s));
+  if (lp.pgrid) DD_CUDA(launch_hist(ctx->hist_mode, lp.pargs, lp.pgrid, lp.psmem, s));
+  if (lp.mgrid) DD_CUDA(launch_mma(lp.margs, lp.mgrid, lp.msmem, s));
+  DD_CUDA(cudaEventRecord(ctx->ev1, s));
+  DD_CUDA(cudaMemcpyAsync(ctx->h_bins, ctx->d_bins, (size_t)lp.nslots * kMaxBins * sizeof(unsigned long long),
                           cudaMemcpyDeviceToHost, s));
+  DD_CUDA(cudaMemcpyAsync(ctx->h_ctl, ctx->d_ctl, kCtlWords * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+  return DD_OK;
+}
+
+// Status word of the last launch (after the stream synchronised).
+static int check_status(dd_context* ctx) {
+  const unsigned st = (unsigned)ctx->h_ctl[2];
+  if (st & 8u) {
+    char buf[256];
+    std::snprintf(buf, sizeof(buf), "self-check: shared access at %llu outside [%llu, %llu), tile %llu",
+                  ctx->h_ctl[4], ctx->h_ctl[5], ctx->h_ctl[6], ctx->h_ctl[7]);
+    set_error(buf);
+    return DD_ERR_CUDA;
+  }
+  if (st & KSTATUS_TIMEOUT) { set_error("a device-side wait timed out"); return DD_ERR_TIMEOUT; }
+  if (st & KSTATUS_BAD_DISTANCE) { set_error("kernel produced a distance outside the bins"); return DD_ERR_CUDA; }
+  if (st & KSTATUS_BAD_JOB) { set_error("kernel saw a tile outside the job table"); return DD_ERR_CUDA; }
   return DD_OK;
 }
 
@@ -209,7 +284,8 @@ int dd_context_create(int device, void* stream, dd_context** out) {
     if (stream) ctx->stream = (cudaStream_t)stream;
     else { e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking); ctx->own_stream = true; }
   }
-  if (e == cudaSuccess) e = cudaMalloc(&ctx->d_counter, sizeof(unsigned long long));
+  if (e == cudaSuccess) e = cudaMalloc(&ctx->d_ctl, kCtlWords * sizeof(unsigned long long));
+  if (e == cudaSuccess) e = cudaMallocHost(&ctx->h_ctl, kCtlWords * sizeof(unsigned long long));
   if (e == cudaSuccess) e = cudaEventCreate(&ctx->ev0);
   if (e == cudaSuccess) e = cudaEventCreate(&ctx->ev1);
   if (e != cudaSuccess) {
@@ -235,7 +311,8 @@ int dd_context_destroy(dd_context* ctx) {
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   if (ctx->gexec) cudaGraphExecDestroy(ctx->gexec);
   if (ctx->d_bins) cudaFree(ctx->d_bins);
-  if (ctx->d_counter) cudaFree(ctx->d_counter);
+  if (ctx->d_ctl) cudaFree(ctx->d_ctl);
+  if (ctx->h_ctl) cudaFreeHost(ctx->h_ctl);
   if (ctx->d_jobs) cudaFree(ctx->d_jobs);
   if (ctx->h_bins) cudaFreeHost(ctx->h_bins);
   if (ctx->h_jobs) cudaFreeHost(ctx->h_jobs);
@@ -258,6 +335,23 @@ int dd_request_shape(const dd_request* req, uint32_t* nbins, uint32_t* h, uint64
   return DD_OK;
 }
 
+int dd_request_plan(const dd_request* req, uint64_t* lattice, uint64_t* tiles, uint64_t* pairs_lo,
+                    uint64_t* pairs_hi) {
+  if (!req) { set_error("req is NULL"); return DD_ERR_INVALID_ARGUMENT; }
+  Shape s;
+  std::string err;
+  int st = derive_shape(*req, s, err);
+  if (st != DD_OK) { set_error(err); return st; }
+  std::vector<Job> jobs;
+  plan_jobs(s, *req, jobs);
+  const u128 p = planned_pairs(s, *req);
+  if (lattice) *lattice = s.lattice;
+  if (tiles) *tiles = jobs[0].tiles;
+  if (pairs_lo) *pairs_lo = (uint64_t)p;
+  if (pairs_hi) *pairs_hi = (uint64_t)(p >> 64);
+  return DD_OK;
+}
+
 int dd_postprocess(const dd_request* req, const uint64_t* raw, uint32_t nraw, dd_result* res) {
   if (!req || !raw || !res) { set_error("NULL argument"); return DD_ERR_INVALID_ARGUMENT; }
   Shape s;
@@ -277,83 +371,63 @@ void dd_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out
   out[0] = o.x; out[1] = o.y; out[2] = o.z; out[3] = o.w;
 }
 
-int dd_histogram(dd_context* ctx, const dd_request* req, dd_result* res) {
-  if (!ctx || !req || !res) { set_error("NULL argument"); return DD_ERR_INVALID_ARGUMENT; }
-  const double t0 = now_ms();
-  Shape s;
-  std::string err;
-  int st = derive_shape(*req, s, err);
-  if (st != DD_OK) { set_error(err); return st; }
-  std::vector<Job> jobs;
-  plan_jobs(s, *req, jobs);
-  st = ensure_capacity(ctx, 1, 1);
-  if (st != DD_OK) return st;
-  LaunchPlan lp;
-  st = plan_launch(ctx, jobs, lp);
-  if (st != DD_OK) return st;
-  st = enqueue_launch(ctx, lp, 1, true);
-  if (st != DD_OK) return st;
-  DD_CUDA(cudaStreamSynchronize(ctx->stream));
-  float ms = 0;
-  DD_CUDA(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
-  std::memset(res, 0, sizeof(*res));
-  uint64_t raw[kMaxBins];
-  for (int i = 0; i < kMaxBins; ++i) raw[i] = ctx->h_bins[i];
-  postprocess(*req, s, raw, *res);
-  fill_pairs(*res, planned_pairs(s, *req));
-  res->kernel_used = DD_KERNEL_POPC;
-  res->kernel_ms = ms;
-  res->user_tag = req->user_tag;
-  res->status = DD_OK;
-  res->total_ms = now_ms() - t0;
-  return DD_OK;
-}
+}  // extern "C"
 
-int dd_batch_run(dd_context* ctx, const dd_request* reqs, uint32_t count, dd_result* results,
-                 const dd_batch_options* opts) {
-  if (!ctx || (!reqs && count) || (!results && count)) { set_error("NULL argument"); return DD_ERR_INVALID_ARGUMENT; }
-  if (count == 0) return DD_OK;
+namespace dd {
+
+// One launch for `count` requests: plan, (graph-)enqueue, synchronise, check
+// the kernels' status word, post-process every request.
+static int run_requests(dd_context* ctx, const dd_request* reqs, uint32_t count, dd_result* results,
+                        bool use_graph) {
   const double t0 = now_ms();
-  const bool use_graph = opts && opts->use_graph;
   std::vector<Shape> shapes(count);
   std::vector<Job> jobs;
+  std::vector<uint32_t> kernels(count);
   jobs.reserve(count);
   for (uint32_t i = 0; i < count; ++i) {
     std::string err;
     int st = derive_shape(reqs[i], shapes[i], err);
-    if (st != DD_OK) { set_error("request " + std::to_string(i) + ": " + err); return st; }
+    if (st != DD_OK) {
+      set_error(count > 1 ? "request " + std::to_string(i) + ": " + err : err);
+      return st;
+    }
     plan_jobs(shapes[i], reqs[i], jobs);
+    kernels[i] = reqs[i].kernel;
   }
   int st = ensure_capacity(ctx, count, count);
   if (st != DD_OK) return st;
   LaunchPlan lp;
-  st = plan_launch(ctx, jobs, lp);
+  st = plan_launch(ctx, jobs, kernels, lp);
   if (st != DD_OK) return st;
   cudaStream_t s = ctx->stream;
   if (use_graph) {
-    bool same = ctx->gexec && ctx->gjobs.size() == jobs.size() && ctx->ggrid == lp.grid && ctx->gsmem == lp.smem &&
-                std::memcmp(ctx->gjobs.data(), jobs.data(), jobs.size() * sizeof(Job)) == 0;
+    const size_t nj = lp.npopc + lp.nmma;
+    const bool same = ctx->gexec && ctx->gjobs.size() == nj && ctx->ggrid[0] == lp.pgrid &&
+                      ctx->ggrid[1] == lp.mgrid && ctx->gsmem[0] == lp.psmem && ctx->gsmem[1] == lp.msmem &&
+                      std::memcmp(ctx->gjobs.data(), ctx->h_jobs, nj * sizeof(Job)) == 0;
     if (!same) {
       if (ctx->gexec) { cudaGraphExecDestroy(ctx->gexec); ctx->gexec = nullptr; }
       cudaGraph_t g = nullptr;
       DD_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-      st = enqueue_launch(ctx, lp, count, true);
+      st = enqueue_launch(ctx, lp);
       cudaError_t ce = cudaStreamEndCapture(s, &g);
       if (st != DD_OK) { if (g) cudaGraphDestroy(g); return st; }
       if (ce != cudaSuccess) return cuda_fail(ce, "cudaStreamEndCapture");
       ce = cudaGraphInstantiate(&ctx->gexec, g, 0);
       cudaGraphDestroy(g);
       if (ce != cudaSuccess) { ctx->gexec = nullptr; return cuda_fail(ce, "cudaGraphInstantiate"); }
-      ctx->gjobs = jobs;
-      ctx->ggrid = lp.grid;
-      ctx->gsmem = lp.smem;
+      ctx->gjobs.assign(ctx->h_jobs, ctx->h_jobs + nj);
+      ctx->ggrid[0] = lp.pgrid; ctx->ggrid[1] = lp.mgrid;
+      ctx->gsmem[0] = lp.psmem; ctx->gsmem[1] = lp.msmem;
     }
     DD_CUDA(cudaGraphLaunch(ctx->gexec, s));
   } else {
-    st = enqueue_launch(ctx, lp, count, true);
+    st = enqueue_launch(ctx, lp);
     if (st != DD_OK) return st;
   }
   DD_CUDA(cudaStreamSynchronize(s));
+  st = check_status(ctx);
+  if (st != DD_OK) return st;
   float ms = 0;
   DD_CUDA(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
   const double total = now_ms() - t0;
@@ -364,13 +438,34 @@ int dd_batch_run(dd_context* ctx, const dd_request* reqs, uint32_t count, dd_res
     for (int b = 0; b < kMaxBins; ++b) raw[b] = ctx->h_bins[(size_t)i * kMaxBins + b];
     postprocess(reqs[i], shapes[i], raw, r);
     fill_pairs(r, planned_pairs(shapes[i], reqs[i]));
-    r.kernel_used = DD_KERNEL_POPC;
+    r.kernel_used = want_mma(ctx, jobs[i], kernels[i]) ? DD_KERNEL_MMA : DD_KERNEL_POPC;
     r.kernel_ms = ms;  // one launch: the whole batch's device time
     r.total_ms = total;
     r.user_tag = reqs[i].user_tag;
     r.status = DD_OK;
   }
   return DD_OK;
+}
+
+}  // namespace dd
+
+extern "C" {
+
+int dd_histogram(dd_context* ctx, const dd_request* req, dd_result* res) {
+  if (!ctx || !req || !res) { set_error("NULL argument"); return DD_ERR_INVALID_ARGUMENT; }
+  return run_requests(ctx, req, 1, res, false);
+}
+
+int dd_batch_run(dd_context* ctx, const dd_request* reqs, uint32_t count, dd_result* results,
+                 const dd_batch_options* opts) {
+  if (!ctx || (!reqs && count) || (!results && count)) { set_error("NULL argument"); return DD_ERR_INVALID_ARGUMENT; }
+  if (count == 0) return DD_OK;
+  if (opts && opts->kernel != DD_KERNEL_AUTO) {
+    std::vector<dd_request> r(reqs, reqs + count);
+    for (auto& q : r) q.kernel = opts->kernel;
+    return run_requests(ctx, r.data(), count, results, opts->use_graph != 0);
+  }
+  return run_requests(ctx, reqs, count, results, opts && opts->use_graph);
 }
 
 int dd_measure_popc_peak(dd_context* ctx, double* popc_per_s) {

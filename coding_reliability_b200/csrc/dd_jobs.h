@@ -56,6 +56,13 @@ struct Job {
   uint32_t pad;
 };
 
+// Status bits a kernel reports back (the word is zeroed before each launch).
+enum : uint32_t {
+  KSTATUS_TIMEOUT = 1u,       // a bounded wait ran out
+  KSTATUS_BAD_DISTANCE = 2u,  // a distance outside the job's bins was produced (and dropped)
+  KSTATUS_BAD_JOB = 4u        // a tile mapped outside the job table
+};
+
 // One launch: the job table and the shared work counter.
 struct LaunchArgs {
   const Job* jobs;
@@ -63,6 +70,7 @@ struct LaunchArgs {
   uint32_t smem_bins;        // bin rows reserved per warp in shared memory
   uint64_t total_tiles;
   unsigned long long* counter;  // global work counter (zeroed before launch)
+  unsigned* status;          // KSTATUS_* bits
   uint32_t use_col_table;    // reserve a per-warp column table
   uint32_t pad;
 };

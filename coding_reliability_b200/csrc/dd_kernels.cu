@@ -28,8 +28,36 @@ namespace dd {
 // ---------------------------------------------------------------------------
 // shared-memory bin increments
 // ---------------------------------------------------------------------------
+#ifdef DD_SELF_CHECK
+// Self-checking build (libcodrel_b200_checked.so): every bin access is range
+// checked against the calling warp's shared-memory region; a violation is
+// recorded (first one wins) and the access is skipped.
+struct CheckState {
+  uint32_t lo, hi;            // this warp's bin region [lo, hi) in the shared window
+  unsigned* status;
+  unsigned long long* record;  // [0] flag, [1] offset, [2] lo, [3] hi, [4] tile
+  unsigned long long tile;
+};
+__device__ __forceinline__ CheckState& check_state() {
+  __shared__ CheckState st[kWarpsPerCta];
+  return st[threadIdx.x >> 5];
+}
+#endif
+
 template <int kMode>
 __device__ __forceinline__ void bump(uint32_t saddr) {
+#ifdef DD_SELF_CHECK
+  {
+    CheckState& cs = check_state();
+    if (saddr < cs.lo || saddr + 4 > cs.hi || (saddr & 3)) {
+      atomicOr(cs.status, 8u);
+      if (atomicCAS(cs.record, 0ull, 1ull) == 0ull) {
+        cs.record[1] = saddr; cs.record[2] = cs.lo; cs.record[3] = cs.hi; cs.record[4] = cs.tile;
+      }
+      return;
+    }
+  }
+#endif
   if constexpr (kMode == HIST_RED) {
     asm volatile("red.shared.add.u32 [%0], 1;" ::"r"(saddr) : "memory");
   } else {
@@ -37,6 +65,14 @@ __device__ __forceinline__ void bump(uint32_t saddr) {
     asm volatile("ld.shared.u32 %0, [%1];" : "=r"(v) : "r"(saddr) : "memory");
     asm volatile("st.shared.u32 [%0], %1;" ::"r"(saddr), "r"(v + 1) : "memory");
   }
+}
+
+// Bump for the generic paths: the bin index is checked against the job's bin
+// count; an out-of-range distance is dropped and reported in the status word.
+template <int kMode>
+__device__ __forceinline__ void bump_checked(uint32_t lane_base, uint32_t d, uint32_t nbins, unsigned* status) {
+  if (d < nbins) bump<kMode>(lane_base + (d << 7));
+  else atomicOr(status, KSTATUS_BAD_DISTANCE);
 }
 
 // Warp-aggregated flush: lane l sums bin rows l and l+32 over the 32 lane
@@ -149,17 +185,18 @@ __device__ __forceinline__ void run_table(const uint32_t (&w)[kRowsPerLane], con
 template <int kMode>
 __device__ __forceinline__ void run_generic(const Job& J, const uint64_t (&w)[kRowsPerLane],
                                             const uint64_t (&ri)[kRowsPerLane], const bool (&rv)[kRowsPerLane],
-                                            uint32_t lane_base, uint64_t c0, uint64_t c1, bool diag) {
+                                            uint32_t lane_base, uint64_t c0, uint64_t c1, bool diag,
+                                            unsigned* status) {
   for (uint64_t j = c0; j < c1; ++j) {
     const uint64_t v = col_value(J, j);
 #pragma unroll
     for (int q = 0; q < kRowsPerLane; ++q)
-      if (rv[q] && (!diag || j > ri[q])) bump<kMode>(lane_base + (popc64(w[q] ^ v) << 7));
+      if (rv[q] && (!diag || j > ri[q])) bump_checked<kMode>(lane_base, popc64(w[q] ^ v), J.nbins, status);
   }
 }
 
 template <int kMode>
-__device__ void pairs_tile(const Job& J, uint64_t lt, uint32_t* wbins, uint32_t* table, int lane) {
+__device__ void pairs_tile(const Job& J, uint64_t lt, uint32_t* wbins, uint32_t* table, int lane, unsigned* status) {
   uint64_t r0, c0, c1;
   bool diag = false;
   if (J.shape == SHAPE_TRIANGLE) {
@@ -198,15 +235,24 @@ __device__ void pairs_tile(const Job& J, uint64_t lt, uint32_t* wbins, uint32_t*
   if (diag) {
     const uint64_t mlo = r0 + 1 > c0 ? r0 + 1 : c0;
     const uint64_t mhi = r0 + kWarpRows < c1 ? r0 + kWarpRows : c1;
-    if (mlo < mhi) run_generic<kMode>(J, w, ri, rv, lane_base, mlo, mhi, true);
+    if (mlo < mhi) run_generic<kMode>(J, w, ri, rv, lane_base, mlo, mhi, true, status);
     cf = mhi > mlo ? mhi : mlo;
     if (cf < c0) cf = c0;
   }
   if (cf >= c1) return;
 
-  if (!all_valid || J.col_kind == COL_LATTICE || (J.wide && J.col_kind != COL_PROGRESSION) ||
+  // The unchecked fast paths need every distance of the tile below nbins: the
+  // widest row or column codeword of the tile must have at most nbins-1 bits.
+  uint32_t wbits = 0;
+#pragma unroll
+  for (int q = 0; q < kRowsPerLane; ++q) wbits = max(wbits, 64u - (uint32_t)__clzll((long long)w[q]));
+  wbits = __reduce_max_sync(0xffffffffu, wbits);
+  if (J.col_kind == COL_PROGRESSION) wbits = max(wbits, 64u - (uint32_t)__clzll((long long)(J.A * (c1 - 1))));
+  const bool fits = wbits < J.nbins;
+
+  if (!all_valid || !fits || J.col_kind == COL_LATTICE || (J.wide && J.col_kind != COL_PROGRESSION) ||
       (J.col_kind == COL_PROGRESSION && J.wide && (J.A >> 32))) {
-    run_generic<kMode>(J, w, ri, rv, lane_base, cf, c1, false);
+    run_generic<kMode>(J, w, ri, rv, lane_base, cf, c1, false, status);
     return;
   }
 
@@ -256,7 +302,7 @@ __device__ void pairs_tile(const Job& J, uint64_t lt, uint32_t* wbins, uint32_t*
 // Monte Carlo tiles: 32 codeword rows x kMcSamplesPerTile samples each.
 // ---------------------------------------------------------------------------
 template <int kMode>
-__device__ void mc_tile(const Job& J, uint64_t lt, uint32_t* wbins, int lane) {
+__device__ void mc_tile(const Job& J, uint64_t lt, uint32_t* wbins, int lane, unsigned* status) {
   const uint64_t chunks = (J.iters + kMcSamplesPerTile - 1) / kMcSamplesPerTile;
   const uint64_t rt = lt / chunks, ch = lt % chunks;
   const uint64_t i = rt * 32 + lane;
@@ -282,21 +328,21 @@ __device__ void mc_tile(const Job& J, uint64_t lt, uint32_t* wbins, int lane) {
         const uint32_t jj = sh == 32 ? 0u : (r[u] >> sh);
         if (J.wide || (J.A >> 32)) {
           const uint64_t v = J.A * (uint64_t)jj;
-          bump<kMode>(lane_base + (popc64(w ^ v) << 7));
+          bump_checked<kMode>(lane_base, popc64(w ^ v), J.nbins, status);
         } else {
-          bump<kMode>(lane_base + (__popc(wl ^ (a * jj)) << 7));
+          bump_checked<kMode>(lane_base, __popc(wl ^ (a * jj)), J.nbins, status);
         }
       }
     }
     (void)wh;
     for (; t < t1; ++t) {
       const uint64_t v = J.A * mc_index(J.seed, i, t, J.n);
-      bump<kMode>(lane_base + (popc64(w ^ v) << 7));
+      bump_checked<kMode>(lane_base, popc64(w ^ v), J.nbins, status);
     }
   } else {
     for (uint64_t t = t0; t < t1; ++t) {
       const uint64_t v = J.A * mc_index(J.seed, i, t, J.n);
-      bump<kMode>(lane_base + (popc64(w ^ v) << 7));
+      bump_checked<kMode>(lane_base, popc64(w ^ v), J.nbins, status);
     }
   }
 }
@@ -305,7 +351,7 @@ __device__ void mc_tile(const Job& J, uint64_t lt, uint32_t* wbins, int lane) {
 // Ext-Hamming weight tiles: 32 lanes x 256 generated messages.
 // ---------------------------------------------------------------------------
 template <int kMode>
-__device__ void weights_tile(const Job& J, uint64_t lt, uint32_t* wbins, int lane) {
+__device__ void weights_tile(const Job& J, uint64_t lt, uint32_t* wbins, int lane, unsigned* status) {
   const uint32_t lane_base = (uint32_t)__cvta_generic_to_shared(wbins) + (uint32_t)lane * 4u;
   const uint64_t g0 = lt * (32ull * 256ull);
 #pragma unroll 4
@@ -324,7 +370,7 @@ __device__ void weights_tile(const Job& J, uint64_t lt, uint32_t* wbins, int lan
       x = g;
       n4 = true;
     }
-    bump<kMode>(lane_base + (popc64(hamming_cw_gpu(x, J.bucket, n4)) << 7));
+    bump_checked<kMode>(lane_base, popc64(hamming_cw_gpu(x, J.bucket, n4)), J.nbins, status);
   }
 }
 
@@ -348,6 +394,16 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32) hist_kernel(LaunchArgs args
   uint32_t* wbins = smem + warp * per_warp;
   uint32_t* table = wbins + args.smem_bins * 32;
   for (uint32_t k = lane; k < args.smem_bins * 32; k += 32) wbins[k] = 0;
+#ifdef DD_SELF_CHECK
+  if (lane == 0) {
+    CheckState& cs = check_state();
+    cs.lo = (uint32_t)__cvta_generic_to_shared(wbins);
+    cs.hi = cs.lo + args.smem_bins * 32 * 4;
+    cs.status = args.status;
+    cs.record = reinterpret_cast<unsigned long long*>(args.status) + 1;
+    cs.tile = 0;
+  }
+#endif
   __syncwarp();
 
   uint32_t cur = 0xffffffffu;
@@ -359,6 +415,11 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32) hist_kernel(LaunchArgs args
     t = __shfl_sync(0xffffffffu, t, 0);
     if (t >= args.total_tiles) break;
     const uint32_t jn = find_job(args.jobs, args.njobs, t);
+    if (jn >= args.njobs || t < args.jobs[jn].tile_begin ||
+        t - args.jobs[jn].tile_begin >= args.jobs[jn].tiles || args.jobs[jn].nbins > args.smem_bins) {
+      if (lane == 0) atomicOr(args.status, KSTATUS_BAD_JOB);
+      continue;
+    }
     if (jn != cur) {
       if (cur != 0xffffffffu && since_flush) flush_bins(wbins, J.bins, J.nbins, lane);
       since_flush = 0;
@@ -366,9 +427,13 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32) hist_kernel(LaunchArgs args
       cur = jn;
     }
     const uint64_t lt = t - J.tile_begin;
-    if (J.kind == JOB_PAIRS) pairs_tile<kMode>(J, lt, wbins, table, lane);
-    else if (J.kind == JOB_MC) mc_tile<kMode>(J, lt, wbins, lane);
-    else weights_tile<kMode>(J, lt, wbins, lane);
+#ifdef DD_SELF_CHECK
+    if (lane == 0) check_state().tile = t;
+    __syncwarp();
+#endif
+    if (J.kind == JOB_PAIRS) pairs_tile<kMode>(J, lt, wbins, table, lane, args.status);
+    else if (J.kind == JOB_MC) mc_tile<kMode>(J, lt, wbins, lane, args.status);
+    else weights_tile<kMode>(J, lt, wbins, lane, args.status);
     if (++since_flush >= kFlushEvery) { flush_bins(wbins, J.bins, J.nbins, lane); since_flush = 0; }
   }
   if (cur != 0xffffffffu && since_flush) flush_bins(wbins, J.bins, J.nbins, lane);

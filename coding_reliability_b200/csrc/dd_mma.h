@@ -1,0 +1,26 @@
+// dd_mma.h — the tcgen05 (5th-gen tensor core) path for AN exhaustive jobs.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstddef>
+#include <cstdint>
+
+#include "dd_jobs.h"
+
+namespace dd {
+
+struct MmaArgs {
+  const Job* jobs;
+  uint32_t njobs;
+  uint32_t hist_rows;        // bin rows in shared memory (max nbins + 1 trash row)
+  uint64_t total_tiles;      // work items: (super tile, 128-row strip) as in the popc kernel
+  unsigned long long* counter;
+  unsigned* status;          // KSTATUS_* bits, zeroed before the launch
+  unsigned long long timeout_ns;  // bound of every mbarrier wait
+};
+
+// True if the job can run on the MMA path (AN exhaustive, codewords <= 60 bits).
+bool mma_eligible(const Job& j);
+size_t mma_smem_bytes(uint32_t hist_rows);
+cudaError_t launch_mma(const MmaArgs& args, int grid, size_t smem, cudaStream_t stream);
+
+}  // namespace dd

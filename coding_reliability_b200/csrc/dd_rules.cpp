@@ -35,10 +35,15 @@ static uint32_t hamming_shard(uint32_t n) {
   }
 }
 
-// Lattice value index (T)(k*step) as the grid kernels compute it.
+// Lattice value index (T)(k*step) as the grid kernels compute it.  The
+// searches below only compare it against limits <= 2^n, and for every k
+// whose product is below 2^32 the uint32 and uint64 casts agree; above that
+// the uint32 cast wraps, which would make the sequence non-monotone, so the
+// comparison uses the exact (non-wrapping) truncation.
 static uint64_t lattice_index(uint64_t k, double step, bool t32) {
+  (void)t32;
   const double x = (double)k * step;
-  return t32 ? (uint64_t)(uint32_t)x : (uint64_t)x;
+  return x >= 18446744073709551615.0 ? ~0ull : (uint64_t)x;
 }
 
 // First k >= lo with (T)(k*step) >= limit (the index sequence is non-decreasing).
@@ -118,7 +123,8 @@ int derive_shape(const dd_request& req, Shape& s, std::string& err) {
         // The unrolled walk could in principle run past the last in-range point
         // (v_k >= A<<n); that never happens for stepsize >= 1, and a point past
         // the range could have n+h+1 set bits, so refuse rather than overflow.
-        if (s.lattice > first_at_or_above(0, N + 2, s.step, s.t32, N)) {
+        if (s.lattice > first_at_or_above(0, N + 2, s.step, s.t32, N) ||
+            (s.lattice && lattice_index(s.lattice - 1, s.step, s.t32) >= N)) {
           err = "1-D grid: lattice walk leaves the codeword range";
           return DD_ERR_UNSUPPORTED;
         }
@@ -128,6 +134,10 @@ int derive_shape(const dd_request& req, Shape& s, std::string& err) {
         s.step2 = 1.0 * (double)N / (double)s.m2;
         s.t32 = (A << req.n) < (1ull << 32);     // an_coding_grid.cu:188
         s.lattice = first_at_or_above(0, N + 2, s.step, s.t32, N);
+        if (lattice_index(s.m2 - 1, s.step2, s.t32) >= N) {
+          err = "2-D grid: row lattice leaves the codeword range";
+          return DD_ERR_UNSUPPORTED;
+        }
       }
     } else {
       if (req.m == 0) { err = "Monte Carlo: m must be > 0"; return DD_ERR_INVALID_ARGUMENT; }

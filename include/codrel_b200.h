@@ -170,6 +170,11 @@ int dd_batch_run(dd_context* ctx, const dd_request* reqs, uint32_t count,
 /* --- host-only helpers (no device needed) ------------------------------- */
 /* Derives nbins/h/A for a request exactly as the reference's drivers do. */
 int dd_request_shape(const dd_request* req, uint32_t* nbins, uint32_t* h, uint64_t* A_eff);
+/* The device work a request plans: lattice points the grid modes visit (the
+ * reference's walk, src/an_coding_grid.cu:78-107), work tiles of the popc
+ * kernel, and distance evaluations (uint128 as lo/hi).  Any pointer may be NULL. */
+int dd_request_plan(const dd_request* req, uint64_t* lattice, uint64_t* tiles, uint64_t* pairs_lo,
+                    uint64_t* pairs_hi);
 /* The reference's post-processing of a raw device histogram into counts[],
  * minb/mincb and the error estimate (the host tail of every run_* driver). */
 int dd_postprocess(const dd_request* req, const uint64_t* raw, uint32_t nraw, dd_result* res);

@@ -30,6 +30,11 @@ def lib() -> C.CDLL:
         L.dd_oracle_an_rows.argtypes = [u64, u32, u64, u64, _u64p, u32]
         L.dd_oracle_an_grid1d.argtypes = [u64, u32, u32, u64, _u64p, u32, _u64p]
         L.dd_oracle_an_grid2d.argtypes = [u64, u32, u64, u64, _u64p, u32]
+        L.dd_oracle_an_low_distance.argtypes = [u64, u32, u32, _u64p, _u64p]
+        L.dd_oracle_grid1d_points.argtypes = [u64, u32, u32, u64]
+        L.dd_oracle_grid1d_points.restype = u64
+        L.dd_oracle_grid2d_points.argtypes = [u64, u32, u64]
+        L.dd_oracle_grid2d_points.restype = u64
         L.dd_oracle_an_mc.argtypes = [u64, u32, u64, u64, _u64p, u32]
         L.dd_oracle_hamming_weights.argtypes = [u32, _u64p, u32]
         L.dd_oracle_hamming_pairs.argtypes = [u32, i32, _u64p, u32]
@@ -103,6 +108,21 @@ def an_grid1d_raw(A: int, n: int, h: int, m: int, nbins: int) -> tuple[list[int]
     b, k = _buf(), (C.c_uint64 * 1)()
     lib().dd_oracle_an_grid1d(A, n, h, m, b, nbins, k)
     return list(b[:nbins]), k[0]
+
+
+def an_low_distance(A: int, n: int, bits: int) -> tuple[int, int]:
+    """Unordered pairs at distance 1 and 2 by bit-flip membership tests."""
+    d1, d2 = (C.c_uint64 * 1)(), (C.c_uint64 * 1)()
+    lib().dd_oracle_an_low_distance(A, n, bits, d1, d2)
+    return d1[0], d2[0]
+
+
+def grid1d_points(A: int, n: int, h: int, m: int) -> int:
+    return lib().dd_oracle_grid1d_points(A, n, h, m)
+
+
+def grid2d_points(A: int, n: int, m: int) -> int:
+    return lib().dd_oracle_grid2d_points(A, n, m)
 
 
 def an_grid2d_raw(A: int, n: int, m: int, m2: int, nbins: int) -> list[int]:

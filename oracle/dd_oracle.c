@@ -96,6 +96,30 @@ void dd_oracle_an_rows(uint64_t A, unsigned n, uint64_t r0, uint64_t r1, uint64_
   }
 }
 
+/* Unordered pairs at distance 1 and 2, found by flipping one or two of the
+ * `bits` low bits of every codeword and testing the result for membership
+ * (a multiple of A below A*2^n).  Independent of any pair enumeration; used
+ * to arbitrate archived results that fail the conservation law. */
+void dd_oracle_an_low_distance(uint64_t A, unsigned n, unsigned bits, uint64_t* d1, uint64_t* d2)
+{
+  const uint64_t N = 1ull << n, lim = A * N;
+  uint64_t c1 = 0, c2 = 0;
+#pragma omp parallel for reduction(+ : c1, c2) schedule(static)
+  for (long long i = 0; i < (long long)N; ++i) {
+    const uint64_t c = A * (uint64_t)i;
+    for (unsigned a = 0; a < bits; ++a) {
+      const uint64_t x1 = c ^ (1ull << a);
+      if (x1 > c && x1 < lim && x1 % A == 0) ++c1;
+      for (unsigned b = a + 1; b < bits; ++b) {
+        const uint64_t x = x1 ^ (1ull << b);
+        if (x > c && x < lim && x % A == 0) ++c2;
+      }
+    }
+  }
+  *d1 = c1;
+  *d2 = c2;
+}
+
 /* ------------------------------------------------------------------ */
 /* AN grid                                                              */
 /* ------------------------------------------------------------------ */
@@ -125,6 +149,33 @@ static uint64_t grid_lattice_count(uint64_t A, unsigned n, double stepsize, int 
                                 : A * CAST_T((double)k * stepsize)) {
   }
 #undef CAST_T
+  return k;
+}
+
+/* Lattice points the 1-D grid kernel visits for (A, n, h, m). */
+uint64_t dd_oracle_grid1d_points(uint64_t A, unsigned n, unsigned h, uint64_t m)
+{
+  const uint64_t N = 1ull << n;
+  if (m > N) m = N;
+  const double step = 1.0 * (double)N / (double)m;
+  return grid_lattice_count(A, n, step, (n + h + 1) <= 32, m <= 16 ? 3 : 16);
+}
+
+/* Lattice points of dancoding_grid_2d's column walk (an_coding_grid.cu:133). */
+uint64_t dd_oracle_grid2d_points(uint64_t A, unsigned n, uint64_t m)
+{
+  const uint64_t N = 1ull << n;
+  if (m > N) m = N;
+  const double step = 1.0 * (double)N / (double)m;
+  const uint64_t Aend = A << n;
+  const int t32 = Aend < (1ull << 32);
+  uint64_t v = 0, k = 0;
+  while (v < Aend) {
+    ++k;
+    uint64_t tv = (uint64_t)((double)k * step);
+    if (t32) tv = (uint32_t)tv;
+    v = A * tv;
+  }
   return k;
 }
 

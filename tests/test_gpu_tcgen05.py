@@ -1,0 +1,59 @@
+"""Parity of the tcgen05 kind::i8 bit-plane MMA path with the oracle and with
+the popc path (through the C-ABI).  Bit-exact: INT32 accumulation of 0/1
+planes is exact, and the accumulator holds the distance itself."""
+import pytest
+
+import coding_reliability_b200 as dd
+import oracle
+from conftest import golden
+
+pytestmark = pytest.mark.gpu
+
+
+def mma_req(A, n, **kw):
+    return dd.Request(dd.CODE_AN, dd.MODE_EXHAUSTIVE, A, n, kernel=dd.KERNEL_MMA, **kw)
+
+
+@pytest.mark.parametrize("A,n", [(641, 10), (641, 12), (61, 9), (3, 11), (58659, 12), (65521, 13), (1, 12)])
+def test_mma_small_vs_oracle(ctx, A, n):
+    req = mma_req(A, n)
+    nb, h, Aeff = dd.request_shape(req)
+    res = ctx.histogram(req)
+    assert res.kernel_used == dd.KERNEL_MMA
+    assert res.raw == oracle.an_exhaustive_raw(Aeff, n, nb)
+
+
+@pytest.mark.parametrize("A,n", [(58659, 16), (61, 16), (641, 16), (58659, 17), (32771, 18)])
+def test_mma_vs_popc(ctx, A, n):
+    """32-bit and wider (>32-bit) codewords: MMA path equals the popc path."""
+    a = ctx.histogram(mma_req(A, n))
+    b = ctx.histogram(dd.Request(dd.CODE_AN, dd.MODE_EXHAUSTIVE, A, n, kernel=dd.KERNEL_POPC))
+    assert a.kernel_used == dd.KERNEL_MMA and b.kernel_used == dd.KERNEL_POPC
+    assert a.raw == b.raw and a.counts == b.counts
+
+
+def test_mma_solutions_h(ctx):
+    for A in (61, 641):
+        sol = golden("solutions.json")[f"solution_an16_A{A}"]
+        res = ctx.histogram(mma_req(A, 16))
+        k = min(len(sol), res.nbins)
+        assert res.counts[:k] == sol[:k]
+
+
+def test_mma_batch_super_a(ctx):
+    from test_gpu_parity import super_a_set
+    As = super_a_set(64)
+    reqs = [mma_req(A, 16, convention=dd.CONV_SUPER_A) for A in As]
+    out = ctx.batch(reqs, use_graph=True)
+    for A, r in list(zip(As, out))[::8]:
+        p = ctx.histogram(dd.Request(dd.CODE_AN, dd.MODE_EXHAUSTIVE, A, 16, kernel=dd.KERNEL_POPC,
+                                     convention=dd.CONV_SUPER_A))
+        assert r.counts == p.counts
+    assert all(r.kernel_used == dd.KERNEL_MMA for r in out)
+
+
+def test_mma_k24_archive_A63877(ctx):
+    """The config-3 shape (40-bit codewords, 41 bins) on the MMA path vs the archive."""
+    case = next(c for c in golden("an_exhaustive.json") if c["A"] == 63877 and c["n"] == 24)
+    res = ctx.histogram(mma_req(63877, 24))
+    assert res.counts == case["counts"]

@@ -206,3 +206,29 @@ def test_philox_library_matches_oracle(lib):
         ctr = tuple(rng.randrange(1 << 32) for _ in range(4))
         key = tuple(rng.randrange(1 << 32) for _ in range(2))
         assert dd.philox4x32_10(ctr, key) == oracle.philox(ctr, key)
+
+
+def _grid_cases():
+    cases = []
+    for n in (8, 10, 12, 16, 20, 24, 28, 31):
+        N = 1 << n
+        for m in sorted({3, 4, 7, 13, 16, 17, 64, 100, 127, 128, 129, 1000, 1001, 4096, 65536, 100001,
+                         N - 1, N, N + 5, N // 2, N // 3}):
+            if 3 <= m:
+                cases.append((61, n, m))
+    return cases + [(58659, 16, 333), (58659, 24, 65536), (1, 24, 400000), (65533, 24, 400000), (3, 9, 512)]
+
+
+@pytest.mark.parametrize("A,n,m", _grid_cases())
+def test_grid_lattice_points_match_reference_walk(lib, A, n, m):
+    """The lattice size comes from a search over k; it must equal the reference's
+    sequential walk (an_coding_grid.cu:78-107) for every m, powers of two included."""
+    req = dd.Request(dd.CODE_AN, dd.MODE_GRID_1D, A, n, m=m)
+    try:
+        nb, h, Aeff = dd.request_shape(req)
+    except dd.DDError:
+        pytest.skip("n+h+1 > 64")
+    plan = dd.request_plan(req)
+    assert plan["lattice"] == oracle.grid1d_points(Aeff, n, h, m)
+    req2 = dd.Request(dd.CODE_AN, dd.MODE_GRID_2D, A, n, m=m, m2=m)
+    assert dd.request_plan(req2)["lattice"] == oracle.grid2d_points(Aeff, n, m)

@@ -68,6 +68,12 @@ class _Res(C.Structure):
                 ("total_ms", C.c_double), ("user_tag", C.c_uint64)]
 
 
+class _Tuning(C.Structure):
+    _fields_ = [("kernel", C.c_uint32), ("hist_mode", C.c_uint32), ("popc_red_pairs_per_s", C.c_double),
+                ("popc_ldst_pairs_per_s", C.c_double), ("mma_pairs_per_s", C.c_double),
+                ("probe_pairs", C.c_uint64)]
+
+
 class _BatchOpts(C.Structure):
     _fields_ = [("use_graph", C.c_uint32), ("kernel", C.c_uint32), ("ctas_per_sm", C.c_uint32),
                 ("reserved", C.c_uint32)]
@@ -145,6 +151,7 @@ def load() -> C.CDLL:
     lib.dd_context_create.argtypes = [i32, vp, C.POINTER(vp)]
     lib.dd_context_destroy.argtypes = [vp]
     lib.dd_histogram.argtypes = [vp, C.POINTER(_Req), C.POINTER(_Res)]
+    lib.dd_histogram_plain.argtypes = [vp, C.POINTER(_Req), C.POINTER(_Res)]
     lib.dd_batch_run.argtypes = [vp, C.POINTER(_Req), u32, C.POINTER(_Res), C.POINTER(_BatchOpts)]
     lib.dd_request_shape.argtypes = [C.POINTER(_Req), C.POINTER(u32), C.POINTER(u32), C.POINTER(C.c_uint64)]
     lib.dd_postprocess.argtypes = [C.POINTER(_Req), C.POINTER(C.c_uint64), u32, C.POINTER(_Res)]
@@ -155,6 +162,7 @@ def load() -> C.CDLL:
     lib.dd_philox4x32_10.argtypes = [C.POINTER(u32), C.POINTER(u32), C.POINTER(u32)]
     lib.dd_philox4x32_10.restype = None
     lib.dd_measure_popc_peak.argtypes = [vp, C.POINTER(C.c_double)]
+    lib.dd_autotune.argtypes = [vp, C.POINTER(_Tuning)]
     _lib = lib
     return lib
 
@@ -240,6 +248,12 @@ class Context:
         _check(load().dd_histogram(self._h, C.byref(req._c()), C.byref(out)))
         return Result._from(out)
 
+    def histogram_plain(self, req: Request) -> Result:
+        """The plain one-launch-per-instance baseline (AN exhaustive only)."""
+        out = _Res()
+        _check(load().dd_histogram_plain(self._h, C.byref(req._c()), C.byref(out)))
+        return Result._from(out)
+
     def batch(self, reqs: list[Request], use_graph: bool = True, kernel: int = KERNEL_AUTO) -> list[Result]:
         n = len(reqs)
         arr = (_Req * n)(*[r._c() for r in reqs])
@@ -247,6 +261,14 @@ class Context:
         opts = _BatchOpts(1 if use_graph else 0, kernel, 0, 0)
         _check(load().dd_batch_run(self._h, arr, n, out, C.byref(opts)))
         return [Result._from(out[i]) for i in range(n)]
+
+    def autotune(self) -> dict:
+        t = _Tuning()
+        _check(load().dd_autotune(self._h, C.byref(t)))
+        return {"kernel": "mma" if t.kernel == KERNEL_MMA else "popc",
+                "hist_mode": "red" if t.hist_mode == 0 else "ldst",
+                "popc_red_pairs_per_s": t.popc_red_pairs_per_s, "popc_ldst_pairs_per_s": t.popc_ldst_pairs_per_s,
+                "mma_pairs_per_s": t.mma_pairs_per_s, "probe_pairs": t.probe_pairs}
 
     def popc_peak(self) -> float:
         v = C.c_double()

@@ -190,10 +190,12 @@ static int enqueue_launch(dd_context* ctx, const LaunchPlan& lp) {
   DD_CUDA(cudaMemcpyAsync(ctx->d_jobs, ctx->h_jobs, njobs * sizeof(Job), cudaMemcpyHostToDevice, s));
   DD_CUDA(cudaMemsetAsync(ctx->d_bins, 0, (size_t)lp.nslots * kMaxBins * sizeof(unsigned long long), s));
   DD_CUDA(cudaMemsetAsync(ctx->d_ctl, 0, kCtlWords * sizeof(unsigned long long), s));
-  DD_CUDA(cudaEventRecord(ctx->ev0, s));
+  // External records: inside a stream capture they become event-record nodes
+  // of the graph, so the kernel time is measurable on every graph replay.
+  DD_CUDA(cudaEventRecordWithFlags(ctx->ev0, s, cudaEventRecordExternal));
   if (lp.pgrid) DD_CUDA(launch_hist(ctx->hist_mode, lp.pargs, lp.pgrid, lp.psmem, s));
   if (lp.mgrid) DD_CUDA(launch_mma(lp.margs, lp.mgrid, lp.msmem, s));
-  DD_CUDA(cudaEventRecord(ctx->ev1, s));
+  DD_CUDA(cudaEventRecordWithFlags(ctx->ev1, s, cudaEventRecordExternal));
   DD_CUDA(cudaMemcpyAsync(ctx->h_bins, ctx->d_bins, (size_t)lp.nslots * kMaxBins * sizeof(unsigned long long),
                           cudaMemcpyDeviceToHost, s));
   DD_CUDA(cudaMemcpyAsync(ctx->h_ctl, ctx->d_ctl, kCtlWords * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
@@ -451,8 +453,58 @@ static int run_requests(dd_context* ctx, const dd_request* reqs, uint32_t count,
 
 extern "C" {
 
+int dd_autotune(dd_context* ctx, dd_tuning* out) {
+  if (!ctx) { set_error("NULL argument"); return DD_ERR_INVALID_ARGUMENT; }
+  dd_request q;
+  std::memset(&q, 0, sizeof(q));
+  q.code = DD_CODE_AN;
+  q.mode = DD_MODE_EXHAUSTIVE;
+  q.A = 65521;
+  q.n = 17;
+  const uint64_t pairs = (1ull << 17) * ((1ull << 17) - 1) / 2;
+  auto best_ms = [&](uint32_t kernel, int mode, double* ms_out) -> int {
+    const int saved_mode = ctx->hist_mode, saved_tuned = ctx->tuned;
+    ctx->hist_mode = mode;
+    ctx->tuned = 1;  // keep AUTO out of the way while probing
+    q.kernel = kernel;
+    double best = 1e30;
+    int st = DD_OK;
+    for (int rep = 0; rep < 3 && st == DD_OK; ++rep) {
+      dd_result r;
+      st = run_requests(ctx, &q, 1, &r, false);
+      if (st == DD_OK && rep > 0 && r.kernel_ms < best) best = r.kernel_ms;
+    }
+    ctx->hist_mode = saved_mode;
+    ctx->tuned = saved_tuned;
+    *ms_out = best;
+    return st;
+  };
+  double red = 0, ldst = 0, mma = 0;
+  int st = best_ms(DD_KERNEL_POPC, HIST_RED, &red);
+  if (st == DD_OK) st = best_ms(DD_KERNEL_POPC, HIST_LDST, &ldst);
+  if (st == DD_OK) st = best_ms(DD_KERNEL_MMA, ctx->hist_mode, &mma);
+  if (st != DD_OK) return st;
+  ctx->hist_mode = red <= ldst ? HIST_RED : HIST_LDST;
+  ctx->tuned = mma < std::min(red, ldst) ? 2 : 1;
+  if (out) {
+    out->kernel = ctx->tuned == 2 ? DD_KERNEL_MMA : DD_KERNEL_POPC;
+    out->hist_mode = (uint32_t)ctx->hist_mode;
+    out->popc_red_pairs_per_s = pairs / (red * 1e-3);
+    out->popc_ldst_pairs_per_s = pairs / (ldst * 1e-3);
+    out->mma_pairs_per_s = pairs / (mma * 1e-3);
+    out->probe_pairs = pairs;
+  }
+  return DD_OK;
+}
+
 int dd_histogram(dd_context* ctx, const dd_request* req, dd_result* res) {
   if (!ctx || !req || !res) { set_error("NULL argument"); return DD_ERR_INVALID_ARGUMENT; }
+  // First large AUTO exhaustive request: let the autotuner pick the kernel.
+  if (!ctx->tuned && req->kernel == DD_KERNEL_AUTO && req->code == DD_CODE_AN &&
+      req->mode == DD_MODE_EXHAUSTIVE && req->n >= 20) {
+    const int st = dd_autotune(ctx, nullptr);
+    if (st != DD_OK) return st;
+  }
   return run_requests(ctx, req, 1, res, false);
 }
 
@@ -460,12 +512,54 @@ int dd_batch_run(dd_context* ctx, const dd_request* reqs, uint32_t count, dd_res
                  const dd_batch_options* opts) {
   if (!ctx || (!reqs && count) || (!results && count)) { set_error("NULL argument"); return DD_ERR_INVALID_ARGUMENT; }
   if (count == 0) return DD_OK;
+  if (!ctx->tuned && count >= 16 && (!opts || opts->kernel == DD_KERNEL_AUTO)) {
+    const int st = dd_autotune(ctx, nullptr);
+    if (st != DD_OK) return st;
+  }
   if (opts && opts->kernel != DD_KERNEL_AUTO) {
     std::vector<dd_request> r(reqs, reqs + count);
     for (auto& q : r) q.kernel = opts->kernel;
     return run_requests(ctx, r.data(), count, results, opts->use_graph != 0);
   }
   return run_requests(ctx, reqs, count, results, opts && opts->use_graph);
+}
+
+int dd_histogram_plain(dd_context* ctx, const dd_request* req, dd_result* res) {
+  if (!ctx || !req || !res) { set_error("NULL argument"); return DD_ERR_INVALID_ARGUMENT; }
+  if (req->code != DD_CODE_AN || req->mode != DD_MODE_EXHAUSTIVE) {
+    set_error("the plain baseline covers AN exhaustive requests only");
+    return DD_ERR_UNSUPPORTED;
+  }
+  const double t0 = now_ms();
+  Shape s;
+  std::string err;
+  int st = derive_shape(*req, s, err);
+  if (st != DD_OK) { set_error(err); return st; }
+  DD_CUDA(cudaSetDevice(ctx->device));
+  // per call, as the reference's driver: allocate and clear the bins, launch
+  // 128 CTAs per SM, copy the bins back, free them
+  unsigned long long* bins = nullptr;
+  DD_CUDA(cudaMalloc(&bins, s.nbins * sizeof(unsigned long long)));
+  cudaError_t e = cudaMemsetAsync(bins, 0, s.nbins * sizeof(unsigned long long), ctx->stream);
+  if (e == cudaSuccess) e = cudaEventRecord(ctx->ev0, ctx->stream);
+  if (e == cudaSuccess) e = launch_plain(s.A, 1ull << s.n, s.nbins, bins, 128 * ctx->num_sms, ctx->stream);
+  if (e == cudaSuccess) e = cudaEventRecord(ctx->ev1, ctx->stream);
+  uint64_t raw[kMaxBins] = {0};
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(raw, bins, s.nbins * sizeof(unsigned long long), cudaMemcpyDeviceToHost, ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  float ms = 0;
+  if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+  cudaFree(bins);
+  if (e != cudaSuccess) return cuda_fail(e, "plain baseline");
+  std::memset(res, 0, sizeof(*res));
+  postprocess(*req, s, raw, *res);
+  fill_pairs(*res, planned_pairs(s, *req));
+  res->kernel_used = DD_KERNEL_POPC;
+  res->kernel_ms = ms;
+  res->user_tag = req->user_tag;
+  res->total_ms = now_ms() - t0;
+  return DD_OK;
 }
 
 int dd_measure_popc_peak(dd_context* ctx, double* popc_per_s) {

@@ -440,6 +440,42 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32) hist_kernel(LaunchArgs args
 }
 
 // ---------------------------------------------------------------------------
+// The plain baseline: one launch per instance, one codeword row per thread in
+// a grid-stride loop, every j > i in an inner loop, a per-thread column of
+// shared-memory bins bumped by load/add/store, and one 64-bit atomic per bin
+// and thread at the end.  This is the straightforward SIMT design the
+// reference uses (dancoding_shared, src/an_coding.cu:50-105), kept as the
+// comparison point for the persistent and batched paths.
+// ---------------------------------------------------------------------------
+constexpr int kPlainThreads = 128;
+
+__global__ void __launch_bounds__(kPlainThreads) plain_an_kernel(uint64_t A, uint64_t N, uint32_t nbins,
+                                                                 unsigned long long* bins) {
+  extern __shared__ uint32_t cnt[];  // nbins x kPlainThreads
+  for (uint32_t k = threadIdx.x; k < nbins * kPlainThreads; k += kPlainThreads) cnt[k] = 0;
+  __syncthreads();
+  uint32_t* mine = cnt + threadIdx.x;
+  for (uint64_t i = (uint64_t)blockIdx.x * kPlainThreads + threadIdx.x; i < N;
+       i += (uint64_t)gridDim.x * kPlainThreads) {
+    const uint64_t w = A * i;
+    for (uint64_t j = i + 1, v = w + A; j < N; ++j, v += A) {
+      const uint32_t d = popc64(w ^ v);
+      if (d < nbins) mine[d * kPlainThreads] += 1;
+    }
+  }
+  __syncthreads();
+  for (uint32_t b = 0; b < nbins; ++b)
+    if (mine[b * kPlainThreads]) atomicAdd(bins + b, (unsigned long long)mine[b * kPlainThreads]);
+}
+
+cudaError_t launch_plain(uint64_t A, uint64_t N, uint32_t nbins, unsigned long long* bins, int grid,
+                         cudaStream_t stream) {
+  plain_an_kernel<<<grid, kPlainThreads, (size_t)nbins * kPlainThreads * sizeof(uint32_t), stream>>>(A, N, nbins,
+                                                                                                   bins);
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
 // POPC issue-rate probe: 8 independent popc chains per thread.
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(256) popc_rate_kernel(uint32_t iters, uint32_t seed, uint32_t* sink) {

@@ -152,6 +152,13 @@ int dd_context_destroy(dd_context* ctx);
  * super-A run_ancoding (super_a/src/an_coding.cu:135). */
 int dd_histogram(dd_context* ctx, const dd_request* req, dd_result* res);
 
+/* The plain one-launch-per-instance baseline for AN exhaustive requests: the
+ * reference's design on this GPU (src/an_coding.cu:50-105 + :276-421): bins
+ * allocated and freed per call, a grid-stride kernel of 128 CTAs per SM with
+ * per-thread shared-memory bins, one launch, a D2H copy.  It is what the
+ * persistent and batched paths are measured against; results are identical. */
+int dd_histogram_plain(dd_context* ctx, const dd_request* req, dd_result* res);
+
 /* --- batch -------------------------------------------------------------- */
 typedef struct dd_batch_options {
   uint32_t use_graph;       /* capture the launch in a CUDA graph and replay it */
@@ -187,6 +194,21 @@ int dd_format_result(const dd_request* req, const dd_result* res, const char* de
 /* Philox4x32-10 (Salmon et al., SC'11), the counter-based generator behind
  * Monte Carlo mode: out = philox(ctr, key). */
 void dd_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);
+
+/* --- autotuning --------------------------------------------------------- */
+typedef struct dd_tuning {
+  uint32_t kernel;            /* dd_kernel chosen for AN exhaustive requests with kernel = AUTO */
+  uint32_t hist_mode;         /* popc path bin increment: 0 = red.shared.add, 1 = load/add/store */
+  double popc_red_pairs_per_s;
+  double popc_ldst_pairs_per_s;
+  double mma_pairs_per_s;
+  uint64_t probe_pairs;       /* pairs of the probe instance each variant ran */
+} dd_tuning;
+
+/* Times every kernel variant on a probe instance (A = 65521, k = 17: 34-bit
+ * codewords, 8.6e9 pairs) on this context's GPU and keeps the fastest for
+ * kernel = AUTO.  Runs by itself before the first large AUTO request. */
+int dd_autotune(dd_context* ctx, dd_tuning* out);
 
 /* --- measurement -------------------------------------------------------- */
 /* Measures the device's POPC issue rate (popc/s) with a dependency-free POPC

@@ -184,18 +184,20 @@ static int plan_launch(dd_context* ctx, std::vector<Job>& jobs, const std::vecto
 
 // Enqueues: job table H2D, bins / counters / status reset, kernels (bracketed
 // by events), bins + status D2H.
-static int enqueue_launch(dd_context* ctx, const LaunchPlan& lp) {
+static int enqueue_launch(dd_context* ctx, const LaunchPlan& lp, bool capturing) {
   cudaStream_t s = ctx->stream;
   const uint32_t njobs = lp.npopc + lp.nmma;
   DD_CUDA(cudaMemcpyAsync(ctx->d_jobs, ctx->h_jobs, njobs * sizeof(Job), cudaMemcpyHostToDevice, s));
   DD_CUDA(cudaMemsetAsync(ctx->d_bins, 0, (size_t)lp.nslots * kMaxBins * sizeof(unsigned long long), s));
   DD_CUDA(cudaMemsetAsync(ctx->d_ctl, 0, kCtlWords * sizeof(unsigned long long), s));
-  // External records: inside a stream capture they become event-record nodes
-  // of the graph, so the kernel time is measurable on every graph replay.
-  DD_CUDA(cudaEventRecordWithFlags(ctx->ev0, s, cudaEventRecordExternal));
+  // Inside a stream capture the records must be external so that they become
+  // event-record nodes of the graph (the kernel time is then measurable on
+  // every replay); outside a capture the flag is not accepted.
+  const unsigned evflags = capturing ? cudaEventRecordExternal : cudaEventRecordDefault;
+  DD_CUDA(cudaEventRecordWithFlags(ctx->ev0, s, evflags));
   if (lp.pgrid) DD_CUDA(launch_hist(ctx->hist_mode, lp.pargs, lp.pgrid, lp.psmem, s));
   if (lp.mgrid) DD_CUDA(launch_mma(lp.margs, lp.mgrid, lp.msmem, s));
-  DD_CUDA(cudaEventRecordWithFlags(ctx->ev1, s, cudaEventRecordExternal));
+  DD_CUDA(cudaEventRecordWithFlags(ctx->ev1, s, evflags));
   DD_CUDA(cudaMemcpyAsync(ctx->h_bins, ctx->d_bins, (size_t)lp.nslots * kMaxBins * sizeof(unsigned long long),
                           cudaMemcpyDeviceToHost, s));
   DD_CUDA(cudaMemcpyAsync(ctx->h_ctl, ctx->d_ctl, kCtlWords * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
@@ -411,7 +413,7 @@ static int run_requests(dd_context* ctx, const dd_request* reqs, uint32_t count,
       if (ctx->gexec) { cudaGraphExecDestroy(ctx->gexec); ctx->gexec = nullptr; }
       cudaGraph_t g = nullptr;
       DD_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-      st = enqueue_launch(ctx, lp);
+      st = enqueue_launch(ctx, lp, true);
       cudaError_t ce = cudaStreamEndCapture(s, &g);
       if (st != DD_OK) { if (g) cudaGraphDestroy(g); return st; }
       if (ce != cudaSuccess) return cuda_fail(ce, "cudaStreamEndCapture");
@@ -424,7 +426,7 @@ static int run_requests(dd_context* ctx, const dd_request* reqs, uint32_t count,
     }
     DD_CUDA(cudaGraphLaunch(ctx->gexec, s));
   } else {
-    st = enqueue_launch(ctx, lp);
+    st = enqueue_launch(ctx, lp, false);
     if (st != DD_OK) return st;
   }
   DD_CUDA(cudaStreamSynchronize(s));

@@ -37,6 +37,7 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 METRIC = "exact pairs/s (AN k=24 exhaustive histogram)"
+NCU_DRAM_BYTES_PER_LAUNCH = 108288  # popc path, measured by ncu (see profiles/)
 UNIT = "pairs/s"
 
 
@@ -246,7 +247,10 @@ def main() -> None:
                    "pairs": P, "parallelism": f"replicas x{world}",
                    "cold_l2": "n/a: codewords generated in registers, no HBM input"},
         "roofline": {"bound": "popc", "achieved": achieved_popc / 1e9, "peak": popc_peak / 1e9, "unit": "Gpopc/s",
-                     "frac": achieved_popc / popc_peak, "traffic": None,
+                     "frac": achieved_popc / popc_peak, "traffic": NCU_DRAM_BYTES_PER_LAUNCH,
+                     "traffic_source": "dram__bytes_read.sum + dram__bytes_write.sum of one hist_kernel launch, "
+                                       "ncu capture at k=20 (profiles/hist_kernel_an_k20_popc.md); the kernel reads "
+                                       "only its job table and writes only its bins, so the figure does not grow with k",
                      "peak_source": "measured live: dependency-free POPC loop on this GPU (dd_measure_popc_peak)"},
         "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": 256, "d2h_bytes_per_step": 64 * 8 * 8},
         "gpu_launches": args.steps,

@@ -163,6 +163,7 @@ def load() -> C.CDLL:
     lib.dd_philox4x32_10.restype = None
     lib.dd_measure_popc_peak.argtypes = [vp, C.POINTER(C.c_double)]
     lib.dd_autotune.argtypes = [vp, C.POINTER(_Tuning)]
+    lib.dd_histogram_noalloc.argtypes = [i32, vp, C.POINTER(_Req), u32, C.POINTER(_Res)]
     _lib = lib
     return lib
 
@@ -274,6 +275,17 @@ class Context:
         v = C.c_double()
         _check(load().dd_measure_popc_peak(self._h, C.byref(v)))
         return v.value
+
+
+def histogram_noalloc(reqs: list[Request], device: int = 0, stream: int | None = None) -> list[Result]:
+    """dd_histogram_noalloc: up to 32 histograms without any device allocation,
+    for callers that may not allocate device memory (see include/codrel_b200.h).
+    Calls that overlap on the same GPU race on the shared scratch."""
+    n = len(reqs)
+    arr = (_Req * max(n, 1))(*[r._c() for r in reqs])
+    out = (_Res * max(n, 1))()
+    _check(load().dd_histogram_noalloc(device, C.c_void_p(stream) if stream else None, arr, n, out))
+    return [Result._from(out[i]) for i in range(n)]
 
 
 _default_ctx: Context | None = None

@@ -23,7 +23,8 @@ BIN = PKG / "bin"
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + ["-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC,-O3", f"-I{ROOT / 'include'}"]
-LIB_SOURCES = ["dd_kernels.cu", "dd_mma.cu", "dd_host.cu", "dd_server.cpp", "dd_rules.cpp", "dd_dropin.cpp"]
+LIB_SOURCES = ["dd_kernels.cu", "dd_mma.cu", "dd_host.cu", "dd_noalloc.cu", "dd_server.cpp", "dd_rules.cpp",
+               "dd_dropin.cpp"]
 HEADERS = ["dd_device.cuh", "dd_jobs.h", "dd_kernels.h", "dd_host.h", "dd_mma.h"]
 TOOLS = {"codrel": "codrel_main.cpp", "codrel_supera": "codrel_supera_main.cpp"}
 

@@ -159,6 +159,22 @@ int dd_histogram(dd_context* ctx, const dd_request* req, dd_result* res);
  * persistent and batched paths are measured against; results are identical. */
 int dd_histogram_plain(dd_context* ctx, const dd_request* req, dd_result* res);
 
+/* --- no device allocation ------------------------------------------------ */
+/* Has no counterpart in the reference.  For callers that cannot allocate
+ * device memory (a host application that owns every device allocation through
+ * its own pool, a plugin inside such a host, a device whose memory is fully
+ * reserved): computes up to 32 histograms in one popc-path launch on `device`
+ * and `stream` (NULL: the default stream) without calling cudaMalloc, cudaFree
+ * or any allocating routine.  The kernel's scratch (bins, job table, work
+ * counter, status word) is one fixed 21 KB __device__ array that every GPU
+ * loading the library holds until exit; more than 32 requests per call are
+ * refused with DD_ERR_INVALID_ARGUMENT.  The first call on a device looks up
+ * the array's device address and should come before any stream capture on that
+ * device.  All calls share the array: calls that overlap on the GPU race and
+ * must be serialised by the caller.  Results equal dd_histogram's; kernel_ms
+ * is 0 (no events are created). */
+int dd_histogram_noalloc(int device, void* stream, const dd_request* reqs, uint32_t count, dd_result* results);
+
 /* --- batch -------------------------------------------------------------- */
 typedef struct dd_batch_options {
   uint32_t use_graph;       /* capture the launch in a CUDA graph and replay it */

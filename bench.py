@@ -260,6 +260,7 @@ def main() -> None:
     }
     if rank == 0 and not args.no_extras:
         line["super_a_sweep_k16"] = super_a_extra(ctx, dd)
+        line["serving"] = serving_extra(dd)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(A)
     ctx.close()
@@ -268,6 +269,68 @@ def main() -> None:
         dist.destroy_process_group()
     if rank == 0:
         print(json.dumps(line), flush=True)
+
+
+def serving_mix(dd, count=48, seed=20261203):
+    """Seeded query mix: A uniform over odd 8..16-bit values, k uniform in
+    {8,12,16,20,24,32}; k<=20 exhaustive; k>=24 either the grid with stride
+    2^(k-16) or Monte Carlo with 2^32..2^36 Philox samples.  The k=32 grid
+    (2^48 pairs, about a minute of device time for one query) is left out of
+    this timed sample and replaced by its Monte Carlo alternative."""
+    import random
+    rng = random.Random(seed)
+    out = []
+    for i in range(count):
+        A = rng.randrange(129, 1 << 16) | 1
+        k = rng.choice([8, 12, 16, 20, 24, 32])
+        if k <= 20:
+            q = dd.Request(dd.CODE_AN, dd.MODE_EXHAUSTIVE, A, k)
+        elif k == 24 and rng.random() < 0.5:
+            q = dd.Request(dd.CODE_AN, dd.MODE_GRID_1D, A, k, m=1 << 16)  # stride 2^(k-16) = 256
+        else:
+            samples = 1 << rng.randrange(32, 37)
+            q = dd.Request(dd.CODE_AN, dd.MODE_MONTE_CARLO, A, k, m=max(1, samples >> k), seed=i + 1)
+        q.user_tag = i
+        out.append(q)
+    return out
+
+
+def serving_extra(dd, rate_per_s=16.0) -> dict:
+    """p50/p99 latency (submit -> result) and aggregate pairs/s of the query
+    server on a seeded Poisson stream of the serving mix."""
+    import random
+    import threading
+    reqs = serving_mix(dd)
+    rng = random.Random(7)
+    with dd.Server(0, round_ms=20) as s:
+        # warm the server (kernel images, autotune-free path)
+        s.wait(s.submit(dd.Request(dd.CODE_AN, dd.MODE_EXHAUSTIVE, 641, 12)), 60)
+        tickets = []
+        t0 = time.perf_counter()
+
+        def client():
+            for q in reqs:
+                tickets.append(s.submit(q))
+                time.sleep(rng.expovariate(rate_per_s))
+
+        th = threading.Thread(target=client)
+        th.start()
+        th.join()
+        results = [s.wait(t, 600) for t in tickets]
+        wall = time.perf_counter() - t0
+        st = s.stats()
+    assert all(code == 0 for code, _ in results)
+    lat = sorted(r.total_ms for _, r in results)
+    pairs = sum(r.pairs for _, r in results)
+
+    def pct(p):
+        return lat[min(len(lat) - 1, max(0, int(-(-p * len(lat) // 1)) - 1))]
+
+    return {"queries": len(reqs), "arrival_rate_per_s": rate_per_s, "p50_ms": pct(0.50), "p99_ms": pct(0.99),
+            "pairs": pairs, "pairs_per_s_wall": pairs / wall, "pairs_per_s_device": st["pairs_per_s"],
+            "rounds": st["rounds"], "wall_s": wall,
+            "mix": "A odd 8-16 bit, k in {8,12,16,20,24,32}; exhaustive k<=20; k>=24 grid stride 2^(k-16) "
+                   "(k=24) or MC 2^32..2^36 samples; k=32 grid left out of the timed sample"}
 
 
 def super_a_set(count=256, seed=20261203):

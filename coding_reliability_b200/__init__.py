@@ -20,7 +20,7 @@ from pathlib import Path
 __all__ = [
     "CODE_AN", "CODE_EXT_HAMMING", "MODE_EXHAUSTIVE", "MODE_GRID_1D", "MODE_GRID_2D", "MODE_MONTE_CARLO",
     "KERNEL_AUTO", "KERNEL_POPC", "KERNEL_MMA", "HAMMING_WEIGHTS", "HAMMING_ALL_PAIRS", "HAMMING_ALL_PAIRS_DISTINCT",
-    "CONV_GPU", "CONV_CPU", "CONV_SUPER_A", "MAX_BINS", "DDError", "Request", "Result", "Context",
+    "CONV_GPU", "CONV_CPU", "CONV_SUPER_A", "MAX_BINS", "DDError", "Request", "Result", "Context", "Server",
     "load", "lib_path", "postprocess", "request_plan", "format_result", "request_shape", "philox4x32_10", "device_count",
     "run_ancoding", "run_ancoding_cpu", "run_ancoding_grid", "run_ancoding_mc", "run_hamming",
     "run_hamming_grid", "run_hamming_mc",
@@ -164,6 +164,13 @@ def load() -> C.CDLL:
     lib.dd_measure_popc_peak.argtypes = [vp, C.POINTER(C.c_double)]
     lib.dd_autotune.argtypes = [vp, C.POINTER(_Tuning)]
     lib.dd_histogram_noalloc.argtypes = [i32, vp, C.POINTER(_Req), u32, C.POINTER(_Res)]
+    lib.dd_server_create.argtypes = [i32, C.c_void_p, C.POINTER(vp)]
+    lib.dd_server_submit.argtypes = [vp, C.POINTER(_Req), C.POINTER(C.c_uint64)]
+    lib.dd_server_poll.argtypes = [vp, C.c_uint64, C.POINTER(_Res), C.POINTER(C.c_int)]
+    lib.dd_server_wait.argtypes = [vp, C.c_uint64, C.c_double, C.POINTER(_Res)]
+    lib.dd_server_cancel.argtypes = [vp, C.c_uint64]
+    lib.dd_server_get_stats.argtypes = [vp, C.c_void_p]
+    lib.dd_server_destroy.argtypes = [vp]
     _lib = lib
     return lib
 
@@ -286,6 +293,76 @@ def histogram_noalloc(reqs: list[Request], device: int = 0, stream: int | None =
     out = (_Res * max(n, 1))()
     _check(load().dd_histogram_noalloc(device, C.c_void_p(stream) if stream else None, arr, n, out))
     return [Result._from(out[i]) for i in range(n)]
+
+
+class _ServerOpts(C.Structure):
+    _fields_ = [("memory_budget_bytes", C.c_uint64), ("max_queue", C.c_uint32), ("round_ms", C.c_uint32),
+                ("dry_run", C.c_uint32), ("inject_alloc_failure", C.c_uint32)]
+
+
+class _ServerStats(C.Structure):
+    _fields_ = [("submitted", C.c_uint64), ("admitted", C.c_uint64), ("completed", C.c_uint64),
+                ("rejected", C.c_uint64), ("cancelled", C.c_uint64), ("rounds", C.c_uint64),
+                ("active", C.c_uint32), ("queued", C.c_uint32), ("slots", C.c_uint32), ("slots_free", C.c_uint32),
+                ("p50_ms", C.c_double), ("p99_ms", C.c_double), ("pairs_per_s", C.c_double),
+                ("busy_ms", C.c_double), ("pairs_lo", C.c_uint64), ("pairs_hi", C.c_uint64)]
+
+
+class Server:
+    """dd_server: continuous-batching query server on one GPU (dry_run: host logic only)."""
+
+    def __init__(self, device: int = 0, memory_budget_bytes: int = 0, max_queue: int = 0, round_ms: int = 0,
+                 dry_run: bool = False, inject_alloc_failure: bool = False):
+        lib = load()
+        h = C.c_void_p()
+        opts = _ServerOpts(memory_budget_bytes, max_queue, round_ms, int(dry_run), int(inject_alloc_failure))
+        _check(lib.dd_server_create(device, C.byref(opts), C.byref(h)))
+        self._h = h
+
+    def submit(self, req: Request) -> int:
+        t = C.c_uint64()
+        _check(load().dd_server_submit(self._h, C.byref(req._c()), C.byref(t)))
+        return t.value
+
+    def poll(self, ticket: int) -> Result | None:
+        out, done = _Res(), C.c_int()
+        _check(load().dd_server_poll(self._h, ticket, C.byref(out), C.byref(done)))
+        return Result._from(out) if done.value else None
+
+    def wait(self, ticket: int, timeout_s: float = -1.0) -> tuple[int, Result]:
+        """(status, result): status is the query's dd_status (0 = done)."""
+        out = _Res()
+        st = load().dd_server_wait(self._h, ticket, timeout_s, C.byref(out))
+        if st in (7, 8):  # timeout / unknown ticket
+            _check(st)
+        return st, Result._from(out)
+
+    def cancel(self, ticket: int) -> None:
+        _check(load().dd_server_cancel(self._h, ticket))
+
+    def stats(self) -> dict:
+        s = _ServerStats()
+        _check(load().dd_server_get_stats(self._h, C.byref(s)))
+        d = {k: getattr(s, k) for k, _ in _ServerStats._fields_}
+        d["pairs"] = (d.pop("pairs_hi") << 64) | d.pop("pairs_lo")
+        return d
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            load().dd_server_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 _default_ctx: Context | None = None

@@ -119,7 +119,7 @@ static bool want_mma(const dd_context* ctx, const Job& j, uint32_t kernel) {
 // Orders the job table (popc jobs first, then MMA jobs), assigns tile ranges
 // and bin slots (slot = request index), and sizes both persistent grids.
 static int plan_launch(dd_context* ctx, std::vector<Job>& jobs, const std::vector<uint32_t>& kernels,
-                       LaunchPlan& lp) {
+                       LaunchPlan& lp, bool own_bins = true) {
   std::vector<Job> table;
   table.reserve(jobs.size());
   for (int pass = 0; pass < 2; ++pass)
@@ -127,7 +127,7 @@ static int plan_launch(dd_context* ctx, std::vector<Job>& jobs, const std::vecto
       const bool m = want_mma(ctx, jobs[i], kernels[i]);
       if ((pass == 1) != m) continue;
       Job j = jobs[i];
-      j.bins = ctx->d_bins + i * kMaxBins;
+      if (own_bins) j.bins = ctx->d_bins + i * kMaxBins;
       table.push_back(j);
     }
   lp.nslots = (uint32_t)jobs.size();
@@ -219,6 +219,35 @@ static int check_status(dd_context* ctx) {
   if (st & KSTATUS_BAD_JOB) { set_error("kernel saw a tile outside the job table"); return DD_ERR_CUDA; }
   return DD_OK;
 }
+
+// One launch over job sub-ranges whose bins live in caller-owned device
+// memory (the server's resident slots): the bins are NOT reset, so successive
+// rounds accumulate; only the control block is reset and read back.
+int launch_round(dd_context* ctx, std::vector<Job>& jobs, const std::vector<uint32_t>& kernels, float* kernel_ms) {
+  int st = ensure_capacity(ctx, 1, (uint32_t)jobs.size());
+  if (st != DD_OK) return st;
+  LaunchPlan lp;
+  st = plan_launch(ctx, jobs, kernels, lp, false);
+  if (st != DD_OK) return st;
+  cudaStream_t s = ctx->stream;
+  const uint32_t njobs = lp.npopc + lp.nmma;
+  DD_CUDA(cudaMemcpyAsync(ctx->d_jobs, ctx->h_jobs, njobs * sizeof(Job), cudaMemcpyHostToDevice, s));
+  DD_CUDA(cudaMemsetAsync(ctx->d_ctl, 0, kCtlWords * sizeof(unsigned long long), s));
+  DD_CUDA(cudaEventRecord(ctx->ev0, s));
+  if (lp.pgrid) DD_CUDA(launch_hist(ctx->hist_mode, lp.pargs, lp.pgrid, lp.psmem, s));
+  if (lp.mgrid) DD_CUDA(launch_mma(lp.margs, lp.mgrid, lp.msmem, s));
+  DD_CUDA(cudaEventRecord(ctx->ev1, s));
+  DD_CUDA(cudaMemcpyAsync(ctx->h_ctl, ctx->d_ctl, kCtlWords * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+  DD_CUDA(cudaStreamSynchronize(s));
+  st = check_status(ctx);
+  if (st != DD_OK) return st;
+  if (kernel_ms) DD_CUDA(cudaEventElapsedTime(kernel_ms, ctx->ev0, ctx->ev1));
+  return DD_OK;
+}
+
+bool uses_mma(const dd_context* ctx, const Job& j, uint32_t kernel) { return want_mma(ctx, j, kernel); }
+void* context_stream(const dd_context* ctx) { return (void*)ctx->stream; }
+int context_device(const dd_context* ctx) { return ctx->device; }
 
 static double now_ms() {
   using namespace std::chrono;

@@ -58,4 +58,12 @@ std::string bits_string(uint64_t v, uint64_t n);  // printbits, src/globals.cpp:
 
 void set_error(const std::string& msg);
 
+// Round launcher of the query server: one launch over job sub-ranges
+// (Job::tile_offset/tiles) whose bins point into caller-owned device memory,
+// accumulated across rounds (the bins are not reset).
+int launch_round(dd_context* ctx, std::vector<Job>& jobs, const std::vector<uint32_t>& kernels, float* kernel_ms);
+bool uses_mma(const dd_context* ctx, const Job& j, uint32_t kernel);
+void* context_stream(const dd_context* ctx);
+int context_device(const dd_context* ctx);
+
 }  // namespace dd

@@ -54,6 +54,8 @@ struct Job {
   uint32_t bucket;           // Ext-Hamming template bucket N (8 for n in {4,8})
   uint32_t shard;            // Ext-Hamming grid: Shards<N>
   uint32_t pad;
+  uint64_t tile_offset;      // first tile of the instance this job covers (a launch may run a
+                             // sub-range [tile_offset, tile_offset + tiles) of the instance)
 };
 
 // Status bits a kernel reports back (the word is zeroed before each launch).

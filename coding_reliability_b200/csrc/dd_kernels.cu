@@ -426,7 +426,7 @@ __global__ void __launch_bounds__(kWarpsPerCta * 32) hist_kernel(LaunchArgs args
       J = args.jobs[jn];
       cur = jn;
     }
-    const uint64_t lt = t - J.tile_begin;
+    const uint64_t lt = t - J.tile_begin + J.tile_offset;
 #ifdef DD_SELF_CHECK
     if (lane == 0) check_state().tile = t;
     __syncwarp();

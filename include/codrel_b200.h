@@ -190,6 +190,49 @@ typedef struct dd_batch_options {
 int dd_batch_run(dd_context* ctx, const dd_request* reqs, uint32_t count,
                  dd_result* results, const dd_batch_options* opts);
 
+/* --- query server (continuous batching) --------------------------------- */
+/* A server admits distance-distribution queries as they arrive.  Each admitted
+ * query holds a resident slot (its uint64 bins and its pair-space cursor) on
+ * the device; a scheduler thread runs rounds, each ONE persistent launch over a
+ * fair share of every active query's remaining tiles, so queries that arrive
+ * while others run join the next round and their work overlaps on the GPU.
+ * Queries beyond the slots wait in a bounded queue; beyond the queue,
+ * dd_server_submit returns DD_ERR_BUSY.  Results are identical to dd_histogram's.
+ * No counterpart in the reference (its drivers run one query per process). */
+typedef struct dd_server dd_server;
+
+typedef struct dd_server_options {
+  uint64_t memory_budget_bytes; /* device bytes for resident query state; 0 = 64 MiB */
+  uint32_t max_queue;           /* queries waiting for a slot before submit refuses; 0 = 1024 */
+  uint32_t round_ms;            /* target device time of one round; 0 = 20 ms */
+  uint32_t dry_run;             /* 1: schedule without a device (rounds advance cursors only,
+                                   results carry zero bins) - for tests of the host logic */
+  uint32_t inject_alloc_failure;/* test hook: 1 = the slot allocation fails */
+} dd_server_options;
+
+typedef struct dd_server_stats {
+  uint64_t submitted, admitted, completed, rejected, cancelled, rounds;
+  uint32_t active, queued, slots, slots_free;
+  double p50_ms, p99_ms;        /* latency from submit to result, completed queries */
+  double pairs_per_s;           /* distance evaluations of completed queries / busy device time */
+  double busy_ms;               /* device time of all rounds */
+  uint64_t pairs_lo, pairs_hi;  /* distance evaluations of completed queries (uint128) */
+} dd_server_stats;
+
+int dd_server_create(int device, const dd_server_options* opts, dd_server** out);
+/* Validates and enqueues; *ticket identifies the query. */
+int dd_server_submit(dd_server* s, const dd_request* req, uint64_t* ticket);
+/* *done = 1 and *res filled once the query finished (res->status tells how). */
+int dd_server_poll(dd_server* s, uint64_t ticket, dd_result* res, int* done);
+/* Blocks up to timeout_s seconds (< 0: no limit); DD_ERR_TIMEOUT if still running. */
+int dd_server_wait(dd_server* s, uint64_t ticket, double timeout_s, dd_result* res);
+/* A client that goes away: a queued query is dropped, an active one stops after
+ * the current round and frees its slot; its result status is DD_ERR_CANCELLED. */
+int dd_server_cancel(dd_server* s, uint64_t ticket);
+int dd_server_get_stats(dd_server* s, dd_server_stats* out);
+/* Stops the scheduler; unfinished queries end with DD_ERR_CANCELLED. */
+int dd_server_destroy(dd_server* s);
+
 /* --- host-only helpers (no device needed) ------------------------------- */
 /* Derives nbins/h/A for a request exactly as the reference's drivers do. */
 int dd_request_shape(const dd_request* req, uint32_t* nbins, uint32_t* h, uint64_t* A_eff);

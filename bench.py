@@ -127,7 +127,7 @@ def cpu_baseline(A: int, budget_s: float = 20.0) -> dict:
     n = 16
     t = run(n)
     # grow the sample (x4 pairs per +1 bit) while it stays inside the budget
-    while t * 4 < budget_s and n < 24:
+    while t * 4 < 1.5 * budget_s and n < 24:
         n += 1
         t = run(n)
     return {"value": pairs_of(n) / t, "unit": UNIT, "cores": os.cpu_count(), "kind": kind,

@@ -261,6 +261,7 @@ def main() -> None:
     if rank == 0 and not args.no_extras:
         line["super_a_sweep_k16"] = super_a_extra(ctx, dd)
         line["serving"] = serving_extra(dd)
+        line["ancandidates"] = candidates_extra(ctx, popc_peak)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(A)
     ctx.close()
@@ -380,6 +381,41 @@ def super_a_extra(ctx, dd) -> dict:
                 "plain_pairs_per_s": P / plain_wall, "plain_kernel_pairs_per_s": P / plain_kernel,
                 "plain_wall_s": plain_wall,
                 "speedup_vs_plain": plain_wall / best["wall_s"]})
+    return out
+
+
+def candidates_extra(ctx, popc_peak: float) -> dict:
+    """Super-A candidate pre-filter (dd_an_candidates) over every cell with A
+    width 14..17 and data width 1..24, checked against the reference tool's
+    golden digests; the reference's own ANcandidates (OpenMP, all host cores)
+    timed on the A-width-15 cells beside the GPU time of the same cells."""
+    import hashlib
+    gold = {(c["k"], c["a"]): c for c in
+            json.loads((ROOT / "tests" / "golden" / "ancandidates.json").read_text())}
+    cells = [(k, a) for a in range(14, 18) for k in range(1, 25)]
+    ctx.an_candidates(8, 14)  # warm-up
+    kernel_ms, evals, popcs, ok, a15_ms = 0.0, 0, 0, True, 0.0
+    for k, a in cells:
+        info, lst = ctx.an_candidates(k, a)
+        kernel_ms += info["kernel_ms"]
+        evals += info["evaluations"]
+        popcs += info["evaluations"] * (2 if k + a + 2 > 32 else 1)
+        if a == 15:
+            a15_ms += info["total_ms"]
+        g = gold[(k, a)]
+        ok &= (info["sdr"], len(lst), hashlib.sha256(",".join(map(str, lst)).encode()).hexdigest()) == \
+            (g["sdr"], g["count"], g["sha256"])
+    out = {"cells": len(cells), "widths": "A 14..17 bits x data 1..24 bits", "kernel_s": kernel_ms * 1e-3,
+           "evaluations": evals, "evaluations_per_s": evals / (kernel_ms * 1e-3),
+           "popc_frac": popcs / (kernel_ms * 1e-3) / popc_peak, "matches_reference_golden": bool(ok),
+           "gpu_a15_s": a15_ms * 1e-3}
+    import oracle
+    if oracle.ref_ancandidates_available():
+        t = time.perf_counter()
+        oracle.ref_ancandidates(15, 15, 1, 24, timeout=900)
+        out["reference_cpu_a15_s"] = time.perf_counter() - t
+        out["reference_cpu_cores"] = os.cpu_count()
+        out["speedup_a15_vs_reference_cpu"] = out["reference_cpu_a15_s"] / out["gpu_a15_s"]
     return out
 
 

@@ -74,6 +74,13 @@ class _Tuning(C.Structure):
                 ("probe_pairs", C.c_uint64)]
 
 
+class _CandRes(C.Structure):
+    _fields_ = [("status", C.c_int32), ("k", C.c_uint32), ("a_bits", C.c_uint32), ("sdr", C.c_uint32),
+                ("num_A", C.c_uint64), ("num_candidates", C.c_uint64), ("evaluations", C.c_uint64),
+                ("kernel_ms", C.c_double),
+                ("total_ms", C.c_double)]
+
+
 class _BatchOpts(C.Structure):
     _fields_ = [("use_graph", C.c_uint32), ("kernel", C.c_uint32), ("ctas_per_sm", C.c_uint32),
                 ("reserved", C.c_uint32)]
@@ -163,6 +170,7 @@ def load() -> C.CDLL:
     lib.dd_philox4x32_10.restype = None
     lib.dd_measure_popc_peak.argtypes = [vp, C.POINTER(C.c_double)]
     lib.dd_autotune.argtypes = [vp, C.POINTER(_Tuning)]
+    lib.dd_an_candidates.argtypes = [vp, u32, u32, C.POINTER(C.c_uint64), C.c_uint64, C.POINTER(_CandRes)]
     lib.dd_histogram_noalloc.argtypes = [i32, vp, C.POINTER(_Req), u32, C.POINTER(_Res)]
     lib.dd_server_create.argtypes = [i32, C.c_void_p, C.POINTER(vp)]
     lib.dd_server_submit.argtypes = [vp, C.POINTER(_Req), C.POINTER(C.c_uint64)]
@@ -282,6 +290,18 @@ class Context:
         v = C.c_double()
         _check(load().dd_measure_popc_peak(self._h, C.byref(v)))
         return v.value
+
+    def an_candidates(self, k: int, a_bits: int, capacity: int | None = None) -> tuple[dict, list[int]]:
+        """dd_an_candidates: the super-A candidates of (k data bits, A width
+        a_bits) as ANcandidates ranks them; returns (summary, ascending A list)."""
+        if capacity is None:
+            capacity = max(1, 1 << max(0, a_bits - 2)) if a_bits <= 26 else 1 << 24
+        buf = (C.c_uint64 * max(1, capacity))()
+        r = _CandRes()
+        _check(load().dd_an_candidates(self._h, k, a_bits, buf, capacity, C.byref(r)))
+        info = {"k": r.k, "a_bits": r.a_bits, "sdr": r.sdr, "num_A": r.num_A, "num_candidates": r.num_candidates,
+                "evaluations": r.evaluations, "kernel_ms": r.kernel_ms, "total_ms": r.total_ms}
+        return info, list(buf[:min(r.num_candidates, capacity)])
 
 
 def histogram_noalloc(reqs: list[Request], device: int = 0, stream: int | None = None) -> list[Result]:

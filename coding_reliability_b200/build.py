@@ -4,6 +4,7 @@ Produces, next to this file:
   libcodrel_b200.so   the C-ABI (include/codrel_b200.h) + C++ drop-in drivers
   bin/codrel          the reference tool's command line (distance_distribution/src/main.cpp)
   bin/codrel_supera   the super-A fork's command line (distance_distribution_super_a/src/main.cpp)
+  bin/ancandidates    the candidate pre-filter's command line (ANcandidates/ANcandidates.cpp)
 
 Everything is compiled for sm_100a only.  Run `python -m coding_reliability_b200.build`.
 """
@@ -23,10 +24,11 @@ BIN = PKG / "bin"
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + ["-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC,-O3", f"-I{ROOT / 'include'}"]
-LIB_SOURCES = ["dd_kernels.cu", "dd_mma.cu", "dd_host.cu", "dd_noalloc.cu", "dd_server.cpp", "dd_rules.cpp",
-               "dd_dropin.cpp"]
+LIB_SOURCES = ["dd_kernels.cu", "dd_mma.cu", "dd_host.cu", "dd_noalloc.cu", "dd_candidates.cu", "dd_server.cpp",
+               "dd_rules.cpp", "dd_dropin.cpp"]
 HEADERS = ["dd_device.cuh", "dd_jobs.h", "dd_kernels.h", "dd_host.h", "dd_mma.h"]
-TOOLS = {"codrel": "codrel_main.cpp", "codrel_supera": "codrel_supera_main.cpp"}
+TOOLS = {"codrel": "codrel_main.cpp", "codrel_supera": "codrel_supera_main.cpp",
+         "ancandidates": "codrel_ancandidates_main.cpp"}
 
 
 def nvcc() -> str:

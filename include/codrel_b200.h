@@ -274,6 +274,30 @@ int dd_autotune(dd_context* ctx, dd_tuning* out);
  * loop on the context's stream. */
 int dd_measure_popc_peak(dd_context* ctx, double* popc_per_s);
 
+/* --- super-A candidates --------------------------------------------------- */
+/* Replaces the worker loop of ANcandidates (ANcandidates/ANcandidates.cpp:35-163,
+ * main :236-301): for every odd A with exactly a_bits bits the smallest
+ * signed-digit weight popcount(A·x XOR 3·A·x) over x in [1, 2^k), and the A
+ * values whose weight is the largest of the range (the candidates). */
+typedef struct dd_candidates_result {
+  int32_t status;
+  uint32_t k;               /* data bits */
+  uint32_t a_bits;          /* bit width of A */
+  uint32_t sdr;             /* the candidates' weight (the reference's |SDR|) */
+  uint64_t num_A;           /* odd A values scanned */
+  uint64_t num_candidates;  /* all candidates, also when more than fit the list */
+  uint64_t evaluations;     /* codewords weighed (the early exit skips the rest) */
+  double kernel_ms;
+  double total_ms;
+} dd_candidates_result;
+
+/* Writes min(num_candidates, capacity) candidates to out_A in ascending order
+ * (the smallest ones when the list is too short).  1 <= k <= 48,
+ * 1 <= a_bits <= 32, k + a_bits <= 61; a_bits = 1 has no odd A (sdr 0, no
+ * candidates), as in the reference. */
+int dd_an_candidates(dd_context* ctx, uint32_t k, uint32_t a_bits, uint64_t* out_A, uint64_t capacity,
+                     dd_candidates_result* res);
+
 #ifdef __cplusplus
 }
 #endif

@@ -61,6 +61,10 @@ def lib() -> C.CDLL:
         L.dd_oracle_post_hamming_weights.argtypes = [u32, i32, _u64p, u32, _u64p, _u64p]
         L.dd_oracle_post_hamming_sampled.argtypes = [i32, u32, i32, u64, _u64p, u32, _u64p, _u64p]
         L.dd_oracle_num_threads.restype = i32
+        L.dd_oracle_naf_min.argtypes = [u64, u32, u32]
+        L.dd_oracle_naf_min.restype = u32
+        L.dd_oracle_an_candidates.argtypes = [u32, u32, _u64p, u64, C.POINTER(u32)]
+        L.dd_oracle_an_candidates.restype = u64
         _lib = L
     return _lib
 
@@ -209,6 +213,20 @@ def threads() -> int:
     return lib().dd_oracle_num_threads()
 
 
+def naf_min(A: int, k: int, floor: int = 0) -> int:
+    """Smallest signed-digit weight of A*x over x in [1, 2^k) (early exit below floor)."""
+    return lib().dd_oracle_naf_min(A, k, floor)
+
+
+def an_candidates(k: int, a: int) -> tuple[int, list[int]]:
+    """(|SDR|, ascending candidates) of one ANcandidates cell."""
+    cap = max(1, 1 << max(0, a - 2))
+    out = (C.c_uint64 * cap)()
+    sdr = C.c_uint32(0)
+    n = lib().dd_oracle_an_candidates(k, a, out, cap, C.byref(sdr))
+    return sdr.value, list(out[:n])
+
+
 # -- the reference's own tool --------------------------------------------------------
 def ref_available() -> bool:
     return (REF_OUT / "ref_codrel").exists()
@@ -222,6 +240,34 @@ def ref_run(args: list[str], cwd: str | None = None, timeout: float = 600) -> st
     if res.returncode != 0:
         raise RuntimeError(f"ref_codrel {' '.join(args)} failed: {res.stderr[-500:]}")
     return res.stdout
+
+
+def ref_ancandidates_available() -> bool:
+    return (REF_OUT / "ref_ancandidates").exists()
+
+
+def ref_ancandidates(amin: int, amax: int, dmin: int, dmax: int, timeout: float = 600) -> str:
+    """stdout of the reference's ANcandidates tool for the given width ranges."""
+    exe = REF_OUT / "ref_ancandidates"
+    res = subprocess.run([str(exe), "-a", str(amin), "-A", str(amax), "-d", str(dmin), "-D", str(dmax)],
+                         capture_output=True, text=True, timeout=timeout)
+    if res.returncode != 0:
+        raise RuntimeError(f"ref_ancandidates failed: {res.stderr[-500:]}")
+    return res.stdout
+
+
+def parse_candidates(text: str) -> dict[tuple[int, int], tuple[int, list[int]]]:
+    """{(k, a): (|SDR|, sorted candidates)} from ANcandidates' stdout."""
+    out = {}
+    for line in text.splitlines():
+        if not line or line.startswith("#"):
+            continue
+        f = line.split("\t")
+        n, k, a, sdr, cnt = (int(x) for x in f[:5])
+        lst = sorted(int(x) for x in f[5].split(",")) if len(f) > 5 and f[5] else []
+        assert n == k + a and cnt == len(lst), line
+        out[(k, a)] = (sdr, lst)
+    return out
 
 
 _ROW = re.compile(r"^\s*(\d+),\s*([0-9.e+]+),")

@@ -1,6 +1,6 @@
 """Builds the checker side: the C restatement (oracle/_build/libdd_oracle.so)
 and, where the reference's sources are present, the reference's own tool
-(oracle/_ref/ref_codrel, ref_codrel_supera) via oracle/ref.mk.
+(oracle/_ref/ref_codrel, ref_codrel_supera, ref_ancandidates) via oracle/ref.mk.
 
 Test infrastructure only; the product never loads anything built here.
 """
@@ -32,7 +32,7 @@ def build_oracle() -> Path:
 
 def build_reference() -> bool:
     """Compiles the reference tool when its sources exist; True if available."""
-    if (REF_OUT / "ref_codrel").exists() and (REF_OUT / "ref_codrel_supera").exists():
+    if all((REF_OUT / b).exists() for b in ("ref_codrel", "ref_codrel_supera", "ref_ancandidates")):
         return True
     if not (REF_SRC / "distance_distribution" / "src" / "main.cpp").exists():
         return False

@@ -17,6 +17,7 @@
  */
 #include <math.h>
 #include <stdint.h>
+#include <stdlib.h>
 #include <string.h>
 #ifdef _OPENMP
 #include <omp.h>
@@ -593,4 +594,59 @@ int dd_oracle_num_threads(void)
 #else
   return 1;
 #endif
+}
+
+/* ------------------------------------------------------------------ */
+/* super-A candidates (ANcandidates)                                    */
+/* ------------------------------------------------------------------ */
+
+/* Smallest signed-digit weight popcount(c ^ 3c) over the codewords c = A*x,
+ * x in [1, 2^k), as worker() scans them (ANcandidates/ANcandidates.cpp:120-138):
+ * the scan stops once the running minimum is below `floor_`, and then returns
+ * that running minimum. */
+unsigned dd_oracle_naf_min(uint64_t A, unsigned k, unsigned floor_)
+{
+  const uint64_t xmax = (1ull << k) - 1ull;
+  unsigned m = 0xffffffffu;
+  uint64_t c = A;
+  for (uint64_t x = 1; x <= xmax && m >= floor_; ++x, c += A) {
+    const unsigned w = popc64(c ^ (3ull * c));
+    if (w < m) m = w;
+  }
+  return m;
+}
+
+/* One (k, a) cell of ANcandidates' main loop (:256-298): every odd A in
+ * [2^(a-1)+1, 2^a-1], the largest minimum weight among them (|SDR|) and the A
+ * values reaching it, written ascending to out (at most cap).  Returns the
+ * number of candidates.  Workers share the best completed minimum as the
+ * early-exit floor, as the reference's do (:124, :140-152). */
+uint64_t dd_oracle_an_candidates(unsigned k, unsigned a, uint64_t* out, uint64_t cap, unsigned* sdr)
+{
+  *sdr = 0;
+  if (a < 2) return 0;
+  const uint64_t minA = (1ull << (a - 1)) + 1ull, numA = 1ull << (a - 2);
+  unsigned char* mins = (unsigned char*)malloc(numA);
+  unsigned best = 0;
+#pragma omp parallel for schedule(dynamic, 16)
+  for (int64_t i = 0; i < (int64_t)numA; ++i) {
+    unsigned floor_;
+#pragma omp atomic read
+    floor_ = best;
+    const unsigned m = dd_oracle_naf_min(minA + 2ull * (uint64_t)i, k, floor_);
+    mins[i] = (unsigned char)m;
+    if (m >= floor_) {
+#pragma omp critical(dd_oracle_naf_best)
+      if (m > best) best = m;
+    }
+  }
+  uint64_t count = 0;
+  for (uint64_t i = 0; i < numA; ++i)
+    if (mins[i] == best) {
+      if (count < cap) out[count] = minA + 2ull * i;
+      ++count;
+    }
+  free(mins);
+  *sdr = best;
+  return count;
 }

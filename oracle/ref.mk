@@ -1,5 +1,6 @@
-# Builds the reference's own `codrel` tool from its unmodified sources, in place
-# where they lie, into oracle/_ref/.  The reference's CMake files target sm_35/37,
+# Builds the reference's own `codrel` tool (and its super-A fork and the
+# ANcandidates pre-filter) from their unmodified sources, in place where they
+# lie, into oracle/_ref/.  The reference's CMake files target sm_35/37,
 # which CUDA 12.9 no longer accepts, so this recipe calls nvcc on the sources
 # directly with sm_100a.  Only the CPU paths (-c, -e 1 -c, -e 2/3/4) are used as
 # checker and CPU baseline; nothing here is linked into the product.
@@ -25,7 +26,7 @@ SUPA_SRCS := $(addprefix $(SUPA)/src/,main.cpp globals.cpp an_coding.cu an_codin
 
 FLAGS := -O3 -std=c++17 -w -gencode arch=compute_100a,code=sm_100a -Xcompiler -fopenmp
 
-all: $(OUT)/ref_codrel $(OUT)/ref_codrel_supera
+all: $(OUT)/ref_codrel $(OUT)/ref_codrel_supera $(OUT)/ref_ancandidates
 
 $(OUT)/ref_codrel: $(CODREL_SRCS)
 	@mkdir -p $(OUT)
@@ -36,3 +37,7 @@ $(OUT)/ref_codrel_supera: $(SUPA_SRCS)
 	$(NVCC) $(FLAGS) -I$(SUPA)/lib/helper -I$(SUPA)/lib/helper/inc -o $@ $^ -lgomp -lrt
 
 .PHONY: all
+
+$(OUT)/ref_ancandidates: $(REF)/ANcandidates/ANcandidates.cpp
+	@mkdir -p $(OUT)
+	g++ -std=c++17 -O3 -w -fopenmp -o $@ $^

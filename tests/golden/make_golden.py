@@ -9,8 +9,12 @@ default /root/reference):
   * distance_distribution/results/superAs/*.txt    super-A sweep minima
   * the reference's own tool built from its sources (oracle/_ref/ref_codrel):
     full stdout of CPU-path runs, used for the results-file layout and counts.
+  * the reference's ANcandidates tool built from its source
+    (oracle/_ref/ref_ancandidates): |SDR|, count and a SHA-256 of the sorted
+    candidate list of every cell with A width 1..17 and data width 1..24
+    (about 5 minutes on 16 cores for the widths 15..17).
 
-Run from the repo root:  python tests/golden/make_golden.py
+Run from the repo root:  python tests/golden/make_golden.py [fixture.json ...]
 """
 from __future__ import annotations
 
@@ -140,15 +144,37 @@ def ref_runs() -> list:
     return out
 
 
+def candidates_digest(lst: list) -> str:
+    import hashlib
+    return hashlib.sha256(",".join(str(a) for a in sorted(lst)).encode()).hexdigest()
+
+
+def ancandidates() -> list:
+    import oracle
+    oracle.build_reference()
+    out = []
+    for amin, amax in ((1, 14), (15, 17)):
+        cells = oracle.parse_candidates(oracle.ref_ancandidates(amin, amax, 1, 24, timeout=3600))
+        for (k, a), (sdr, lst) in sorted(cells.items(), key=lambda kv: (kv[0][1], kv[0][0])):
+            out.append({"k": k, "a": a, "sdr": sdr, "count": len(lst), "sha256": candidates_digest(lst),
+                        "candidates": lst if len(lst) <= 16 else None})
+    return out
+
+
+FIXTURES = {
+    "solutions.json": solutions,
+    "an_exhaustive.json": an_exhaustive,
+    "an_grid1d.json": an_grid,
+    "super_a.json": super_a,
+    "ref_runs.json": ref_runs,
+    "ancandidates.json": ancandidates,
+}
+
+
 def main() -> None:
-    fixtures = {
-        "solutions.json": solutions(),
-        "an_exhaustive.json": an_exhaustive(),
-        "an_grid1d.json": an_grid(),
-        "super_a.json": super_a(),
-        "ref_runs.json": ref_runs(),
-    }
-    for name, data in fixtures.items():
+    names = sys.argv[1:] or list(FIXTURES)
+    for name in names:
+        data = FIXTURES[name]()
         (HERE / name).write_text(json.dumps(data, indent=0, sort_keys=True))
         print(name, (HERE / name).stat().st_size, "bytes")
 

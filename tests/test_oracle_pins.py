@@ -129,3 +129,40 @@ def test_mc_index_layout():
     assert oracle.mc_index(seed, idx, 5, 32) == o2[1]
     # two 64-bit samples per block for n > 32
     assert oracle.mc_index(seed, idx, 1, 40) == ((o[2] << 32) | o[3]) >> 24
+
+
+def _digest(lst):
+    import hashlib
+    return hashlib.sha256(",".join(str(a) for a in lst).encode()).hexdigest()
+
+
+def test_candidates_oracle_vs_reference_golden():
+    """ANcandidates cells (A width 1..14, data width 1..20) from the reference's
+    own tool, against the oracle's restatement of its worker."""
+    n = 0
+    for c in golden("ancandidates.json"):
+        if c["a"] > 14 or c["k"] > 20:
+            continue
+        sdr, lst = oracle.an_candidates(c["k"], c["a"])
+        assert (sdr, len(lst), _digest(lst)) == (c["sdr"], c["count"], c["sha256"]), (c["k"], c["a"])
+        if c["candidates"] is not None:
+            assert lst == c["candidates"]
+        n += 1
+    assert n == 14 * 20
+
+
+def test_candidates_reference_tool_live():
+    if not oracle.ref_ancandidates_available():
+        pytest.skip("reference ANcandidates not built")
+    cells = oracle.parse_candidates(oracle.ref_ancandidates(2, 11, 1, 14))
+    assert len(cells) == 10 * 14
+    for (k, a), want in cells.items():
+        assert oracle.an_candidates(k, a) == want
+
+
+def test_naf_weight_early_exit():
+    # the worker's early exit returns the running minimum once it is below the floor
+    exact = oracle.naf_min(58659, 16)
+    assert exact == 6
+    assert oracle.naf_min(58659, 16, floor=exact) == exact
+    assert oracle.naf_min(58659, 16, floor=exact + 1) < exact + 1

@@ -170,6 +170,7 @@ def load() -> C.CDLL:
     lib.dd_philox4x32_10.restype = None
     lib.dd_measure_popc_peak.argtypes = [vp, C.POINTER(C.c_double)]
     lib.dd_autotune.argtypes = [vp, C.POINTER(_Tuning)]
+    lib.dd_mc_extend.argtypes = [vp, C.POINTER(_Req), C.c_uint64, C.POINTER(C.c_uint64), C.POINTER(_Res)]
     lib.dd_an_candidates.argtypes = [vp, u32, u32, C.POINTER(C.c_uint64), C.c_uint64, C.POINTER(_CandRes)]
     lib.dd_histogram_noalloc.argtypes = [i32, vp, C.POINTER(_Req), u32, C.POINTER(_Res)]
     lib.dd_server_create.argtypes = [i32, C.c_void_p, C.POINTER(vp)]
@@ -262,6 +263,14 @@ class Context:
     def histogram(self, req: Request) -> Result:
         out = _Res()
         _check(load().dd_histogram(self._h, C.byref(req._c()), C.byref(out)))
+        return Result._from(out)
+
+    def mc_extend(self, req: Request, it_done: int, raw_done: list[int]) -> Result:
+        """dd_mc_extend: `req` (Monte Carlo, req.m samples per codeword) grown
+        from an earlier run of it_done samples whose raw bins are raw_done."""
+        raw = (C.c_uint64 * 64)(*(list(raw_done) + [0] * (64 - len(raw_done))))
+        out = _Res()
+        _check(load().dd_mc_extend(self._h, C.byref(req._c()), it_done, raw, C.byref(out)))
         return Result._from(out)
 
     def histogram_plain(self, req: Request) -> Result:

@@ -174,7 +174,10 @@ static void ancoding_search_super_A() {
             << (n <= 16 ? ",exact" : ",grid") << std::endl;
 }
 
-// src/main.cpp:179-202.
+// src/main.cpp:179-202, with one difference: each step continues from the
+// previous step's samples (run_ancoding_mc_continue draws only the new ones;
+// the histogram equals a fresh run with the step's iterations), so a step's
+// times are those of its new samples.
 static void ancoding_mc_search() {
   int step = 0;
   double cur_err = 1.0;
@@ -183,8 +186,9 @@ static void ancoding_mc_search() {
   std::printf("AN-Coding MonteCarlo starting with %llu iterations\n", nr_iterations);
   FILE* f = std::fopen("ancoding_mc_search.csv", "w");
   double times[2];
+  McSearchState state;
   while (true) {
-    cur_err = run_ancoding_mc(g_flags.n, nr_iterations, g_flags.A, 0, times, nullptr, nullptr, 0, g_flags.nr_dev);
+    cur_err = run_ancoding_mc_continue(g_flags.n, nr_iterations, g_flags.A, times, state);
     std::printf("%llu iterations - max. rel. error %lf\n", nr_iterations, cur_err);
     if (f)
       std::fprintf(f, "%d,%llu,%lf,%llu,%lf,%lf,%lf\n", step, g_flags.n, g_flags.mc_search_bound, nr_iterations,

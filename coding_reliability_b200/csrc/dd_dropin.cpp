@@ -263,6 +263,19 @@ double run_ancoding_mc(uintll_t n, uintll_t iterations, uintll_t A, int verbose,
   return r.max_rel_error;
 }
 
+double run_ancoding_mc_continue(uintll_t n, uintll_t iterations, uintll_t A, double* times, McSearchState& state) {
+  dd_request q = make_request(DD_CODE_AN, DD_MODE_MONTE_CARLO, A, (uint32_t)n);
+  q.m = iterations;
+  q.seed = kSeedAnMc;
+  dd_result r;
+  int st = dd_mc_extend(shared_context(), &q, state.it_done, state.raw, &r);
+  if (st != DD_OK) throw std::runtime_error(std::string("codrel_b200: ") + dd_last_error());
+  state.it_done = r.iterations;
+  for (int b = 0; b < DD_MAX_BINS; ++b) state.raw[b] = r.raw[b];
+  fill_times(r, times);
+  return r.max_rel_error;
+}
+
 void run_hamming(uintll_t n, int with_1bit, int file_output, int nr_dev) {
   (void)nr_dev;
   hamming_common(n, with_1bit, file_output, DD_HAMMING_WEIGHTS, "hamming_gpu", true, false, "");

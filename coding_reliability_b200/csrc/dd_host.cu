@@ -410,8 +410,15 @@ namespace dd {
 
 // One launch for `count` requests: plan, (graph-)enqueue, synchronise, check
 // the kernels' status word, post-process every request.
+// `continued` (Monte Carlo continuation, one request): draw only the samples
+// [continued->it_done, m) and add continued->raw_done to the device bins.
+struct McContinuation {
+  uint64_t it_done;
+  const uint64_t* raw_done;
+};
+
 static int run_requests(dd_context* ctx, const dd_request* reqs, uint32_t count, dd_result* results,
-                        bool use_graph) {
+                        bool use_graph, const McContinuation* continued = nullptr) {
   const double t0 = now_ms();
   std::vector<Shape> shapes(count);
   std::vector<Job> jobs;
@@ -426,6 +433,11 @@ static int run_requests(dd_context* ctx, const dd_request* reqs, uint32_t count,
     }
     plan_jobs(shapes[i], reqs[i], jobs);
     kernels[i] = reqs[i].kernel;
+  }
+  if (continued) {
+    Job& j = jobs[0];
+    j.sample_begin = continued->it_done;
+    j.tiles = job_tiles(j);
   }
   int st = ensure_capacity(ctx, count, count);
   if (st != DD_OK) return st;
@@ -469,8 +481,13 @@ static int run_requests(dd_context* ctx, const dd_request* reqs, uint32_t count,
     std::memset(&r, 0, sizeof(r));
     uint64_t raw[kMaxBins];
     for (int b = 0; b < kMaxBins; ++b) raw[b] = ctx->h_bins[(size_t)i * kMaxBins + b];
+    u128 pairs = planned_pairs(shapes[i], reqs[i]);
+    if (continued) {
+      for (uint32_t b = 0; b < shapes[i].nbins; ++b) raw[b] += continued->raw_done[b];
+      pairs = (u128)(1ull << shapes[i].n) * (shapes[i].m - continued->it_done);
+    }
     postprocess(reqs[i], shapes[i], raw, r);
-    fill_pairs(r, planned_pairs(shapes[i], reqs[i]));
+    fill_pairs(r, pairs);
     r.kernel_used = want_mma(ctx, jobs[i], kernels[i]) ? DD_KERNEL_MMA : DD_KERNEL_POPC;
     r.kernel_ms = ms;  // one launch: the whole batch's device time
     r.total_ms = total;
@@ -553,6 +570,32 @@ int dd_batch_run(dd_context* ctx, const dd_request* reqs, uint32_t count, dd_res
     return run_requests(ctx, r.data(), count, results, opts->use_graph != 0);
   }
   return run_requests(ctx, reqs, count, results, opts && opts->use_graph);
+}
+
+int dd_mc_extend(dd_context* ctx, const dd_request* req, uint64_t it_done, const uint64_t* raw_done, dd_result* res) {
+  if (!ctx || !req || !res || (it_done && !raw_done)) { set_error("NULL argument"); return DD_ERR_INVALID_ARGUMENT; }
+  if (req->code != DD_CODE_AN || req->mode != DD_MODE_MONTE_CARLO) {
+    set_error("dd_mc_extend: AN Monte Carlo requests only");
+    return DD_ERR_UNSUPPORTED;
+  }
+  Shape s;
+  std::string err;
+  int st = derive_shape(*req, s, err);
+  if (st != DD_OK) { set_error(err); return st; }
+  if (it_done > s.m) {
+    set_error("dd_mc_extend: more samples done than requested (after capping at 2^n)");
+    return DD_ERR_INVALID_ARGUMENT;
+  }
+  if (it_done == s.m) {  // nothing left to draw: post-process what the caller has
+    uint64_t raw[kMaxBins] = {0};
+    for (uint32_t b = 0; b < s.nbins; ++b) raw[b] = raw_done[b];
+    std::memset(res, 0, sizeof(*res));
+    postprocess(*req, s, raw, *res);
+    res->user_tag = req->user_tag;
+    return DD_OK;
+  }
+  const McContinuation c{it_done, raw_done};
+  return run_requests(ctx, req, 1, res, false, &c);
 }
 
 int dd_histogram_plain(dd_context* ctx, const dd_request* req, dd_result* res) {

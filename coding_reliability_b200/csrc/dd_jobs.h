@@ -56,6 +56,7 @@ struct Job {
   uint32_t pad;
   uint64_t tile_offset;      // first tile of the instance this job covers (a launch may run a
                              // sub-range [tile_offset, tile_offset + tiles) of the instance)
+  uint64_t sample_begin;     // MC: every codeword draws its samples [sample_begin, iters) only
 };
 
 // Status bits a kernel reports back (the word is zeroed before each launch).

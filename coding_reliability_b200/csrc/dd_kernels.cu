@@ -303,11 +303,11 @@ __device__ void pairs_tile(const Job& J, uint64_t lt, uint32_t* wbins, uint32_t*
 // ---------------------------------------------------------------------------
 template <int kMode>
 __device__ void mc_tile(const Job& J, uint64_t lt, uint32_t* wbins, int lane, unsigned* status) {
-  const uint64_t chunks = (J.iters + kMcSamplesPerTile - 1) / kMcSamplesPerTile;
+  const uint64_t chunks = (J.iters - J.sample_begin + kMcSamplesPerTile - 1) / kMcSamplesPerTile;
   const uint64_t rt = lt / chunks, ch = lt % chunks;
   const uint64_t i = rt * 32 + lane;
   if (i >= J.rows) return;
-  const uint64_t t0 = ch * kMcSamplesPerTile;
+  const uint64_t t0 = J.sample_begin + ch * kMcSamplesPerTile;
   const uint64_t t1 = t0 + kMcSamplesPerTile < J.iters ? t0 + kMcSamplesPerTile : J.iters;
   const uint32_t lane_base = (uint32_t)__cvta_generic_to_shared(wbins) + (uint32_t)lane * 4u;
   const uint64_t w = J.A * i;
@@ -318,7 +318,13 @@ __device__ void mc_tile(const Job& J, uint64_t lt, uint32_t* wbins, int lane, un
     const uint32_t wl = (uint32_t)w, wh = (uint32_t)(w >> 32);
     const uint32_t a = (uint32_t)J.A;
     uint64_t t = t0;
-    // whole Philox blocks (t0 is a multiple of 4)
+    // up to the next Philox block boundary (t0 is not a multiple of 4 when a
+    // continued run starts inside a block)
+    for (; t < t1 && (t & 3); ++t) {
+      const uint64_t v = J.A * mc_index(J.seed, i, t, J.n);
+      bump_checked<kMode>(lane_base, popc64(w ^ v), J.nbins, status);
+    }
+    // whole Philox blocks
     for (; t + 4 <= t1; t += 4) {
       const uint64_t blk = t >> 2;
       const Philox4 o = philox4x32_10((uint32_t)blk, (uint32_t)(blk >> 32), i0, i1, k0, k1);

@@ -175,6 +175,16 @@ int dd_histogram_plain(dd_context* ctx, const dd_request* req, dd_result* res);
  * is 0 (no events are created). */
 int dd_histogram_noalloc(int device, void* stream, const dd_request* reqs, uint32_t count, dd_result* results);
 
+/* Monte Carlo continued (AN codes): the result of `req` (req->m samples per
+ * codeword) computed from the first it_done samples, whose device histogram
+ * the caller passes in raw_done (dd_result.raw of the earlier run with
+ * m = it_done, same A, n and seed), plus only the samples [it_done, req->m).
+ * A codeword's t-th sample depends on (seed, codeword, t) alone, so the result
+ * is bit-identical to dd_histogram(req).  This lets an error-bound search
+ * (the reference's ancoding_mc_search, src/main.cpp:179-202, which restarts
+ * with 3x the iterations) grow the sample count without redrawing. */
+int dd_mc_extend(dd_context* ctx, const dd_request* req, uint64_t it_done, const uint64_t* raw_done, dd_result* res);
+
 /* --- batch -------------------------------------------------------------- */
 typedef struct dd_batch_options {
   uint32_t use_graph;       /* capture the launch in a CUDA graph and replay it */

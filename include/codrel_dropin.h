@@ -33,6 +33,16 @@ void run_ancoding_cpu(uintll_t n, uintll_t A, int verbose, double* times, uintll
 double run_hamming_mc(uintll_t n, int with_1bit, uintll_t iterations, int file_output, int nr_dev);
 double run_ancoding_mc(uintll_t n, uintll_t iterations, uintll_t A, int verbose, double* times, uintll_t* minb,
                        uint128_t* mincb, int file_output, int nr_dev);
+/* Addition without a counterpart in the reference: the Monte Carlo step of the
+ * error-bound search (src/main.cpp:179-202) that continues from the previous
+ * step's samples instead of redrawing them (dd_mc_extend).  `state` starts
+ * zeroed; each call grows it to `iterations` samples per codeword.  Returns the
+ * same max. rel. error as run_ancoding_mc(n, iterations, A, ...) would. */
+struct McSearchState {
+  uintll_t it_done = 0;
+  uint64_t raw[DD_MAX_BINS] = {0};
+};
+double run_ancoding_mc_continue(uintll_t n, uintll_t iterations, uintll_t A, double* times, McSearchState& state);
 double run_ancoding_grid(int gdim, uintll_t n, uintll_t iterations, uintll_t iterations2, uintll_t A, int verbose,
                          double* times, uintll_t* minb, uint128_t* mincb, int file_output, int nr_dev);
 double run_hamming_grid(uintll_t n, int with_1bit, uintll_t iterations, int file_output, int nr_dev);

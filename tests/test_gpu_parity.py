@@ -135,8 +135,12 @@ def test_an_grid1d_oracle(ctx, A, n, m):
     assert res.raw == raw
 
 
-@pytest.mark.parametrize("A,n,m,m2", [(61, 12, 100, 37), (641, 14, 64, 64), (58659, 18, 50, 300), (3, 8, 256, 1)])
+@pytest.mark.parametrize("A,n,m,m2", [(61, 12, 100, 37), (641, 14, 64, 64), (58659, 18, 50, 300), (3, 8, 256, 1),
+                                      (61, 40, 1000, 1000), (58659, 40, 4096, 512), (61, 48, 2000, 3000),
+                                      (255, 48, 1 << 16, 7), (641, 36, 999, 1001)])
 def test_an_grid2d_oracle(ctx, A, n, m, m2):
+    """Includes the k=40 and k=48 buckets (an_coding.h:27-29,38-40): 2^(2k)/(m*m2)
+    scale factors above 2^64, so the uint128 counts are exercised."""
     req = dd.Request(dd.CODE_AN, dd.MODE_GRID_2D, A, n, m=m, m2=m2)
     nb, h, Aeff = dd.request_shape(req)
     res = ctx.histogram(req)
@@ -157,6 +161,19 @@ def test_an_mc_replay(ctx, A, n, it, seed):
     res = ctx.histogram(req)
     assert res.raw == oracle.an_mc_raw(Aeff, n, it, seed, nb)
     assert res.counts == oracle.an_mc_counts(n, min(it, 1 << n), res.raw)
+
+
+@pytest.mark.parametrize("A,n,it", [(61, 40, 1), (641, 36, 2)])
+def test_an_mc_wide_buckets(ctx, A, n, it):
+    """k=36/40 Monte Carlo (2^k codewords x it samples; too long to replay on the
+    CPU): every sample lands in a bin, and the uint128 counts are the host
+    post-processing of the device bins."""
+    req = dd.Request(dd.CODE_AN, dd.MODE_MONTE_CARLO, A, n, m=it, seed=3)
+    nb, h, Aeff = dd.request_shape(req)
+    res = ctx.histogram(req)
+    assert sum(res.raw) == (1 << n) * it
+    assert res.counts == oracle.an_mc_counts(n, it, res.raw)
+    assert max(res.counts) > (1 << 64)
 
 
 def test_an_mc_statistical_agreement(ctx):

@@ -173,6 +173,26 @@ def reference_arm(args) -> None:
 
 
 # ------------------------------------------------------------------------------------
+# replicas: one full instance per rank, no collective on the data path
+# ------------------------------------------------------------------------------------
+def max_over_ranks(values: list[float], world: int, device: str) -> list[float]:
+    """Each value's maximum over all ranks (the slowest replica's times)."""
+    if world == 1:
+        return list(values)
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor(values, dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return t.tolist()
+
+
+def replica_throughput(units_per_rank: int, world: int, slowest_ms: float) -> float:
+    """Whole-job throughput: every rank processed units_per_rank units, the job
+    ends with the slowest rank."""
+    return units_per_rank * world / (slowest_ms * 1e-3)
+
+
+# ------------------------------------------------------------------------------------
 # the B200 arm
 # ------------------------------------------------------------------------------------
 def main() -> None:
@@ -225,18 +245,13 @@ def main() -> None:
     total_ms = ev0.elapsed_time(ev1)
     clk = clocks.stop()
 
-    t_kernel, t_total = kernel_ms, total_ms
-    if world > 1:
-        import torch.distributed as dist
-        t = torch.tensor([t_kernel, t_total], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_kernel, t_total = t.tolist()
+    t_kernel, t_total = max_over_ranks([kernel_ms, total_ms], world, "cuda")
     # every step must produce the same exact histogram
     assert all(r.counts == results[0].counts for r in results)
     assert sum(results[0].raw) == P
 
-    value = P * args.steps * world / (t_kernel * 1e-3)
-    e2e = P * args.steps * world / (t_total * 1e-3)
+    value = replica_throughput(P * args.steps, world, t_kernel)
+    e2e = replica_throughput(P * args.steps, world, t_total)
     per_gpu = P * args.steps / (kernel_ms * 1e-3)
     achieved_popc = per_gpu * 1.0  # one 32-bit POPC per pair (high word folded per segment)
     line = {

@@ -18,6 +18,27 @@ constexpr int kTileCols = 1024;     // columns per warp tile
 constexpr int kSuper = 1024;        // triangle super-tile side
 constexpr int kStrips = kSuper / kWarpRows;    // warp tiles per super tile (8)
 constexpr int kMcSamplesPerTile = 256;         // Monte Carlo: samples per lane per tile
+constexpr uint64_t kMcMaxRowsPerLane = 64;     // Monte Carlo: codewords per lane per tile (few samples each)
+
+#if defined(__CUDACC__)
+#define DD_HOST_DEVICE __host__ __device__
+#else
+#define DD_HOST_DEVICE
+#endif
+
+// Monte Carlo tile shape, shared by the host (tile counts) and the kernel: with
+// `spl` samples per codeword to draw, a lane takes one codeword and up to
+// kMcSamplesPerTile of its samples, or, when spl is smaller than that, several
+// codewords with all their samples, so that every tile holds about
+// 32 x kMcSamplesPerTile samples.
+DD_HOST_DEVICE inline uint64_t mc_rows_per_lane(uint64_t spl) {
+  if (spl >= (uint64_t)kMcSamplesPerTile) return 1;
+  const uint64_t r = (uint64_t)kMcSamplesPerTile / (spl ? spl : 1);
+  return r < kMcMaxRowsPerLane ? r : kMcMaxRowsPerLane;
+}
+DD_HOST_DEVICE inline uint64_t mc_chunks(uint64_t spl) {
+  return spl >= (uint64_t)kMcSamplesPerTile ? (spl + kMcSamplesPerTile - 1) / kMcSamplesPerTile : 1;
+}
 constexpr uint32_t kFlushEvery = 1u << 16;     // warp tiles between flushes (uint32 counter bound)
 
 enum JobKind : uint32_t {

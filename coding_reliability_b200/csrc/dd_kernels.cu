@@ -299,57 +299,135 @@ __device__ void pairs_tile(const Job& J, uint64_t lt, uint32_t* wbins, uint32_t*
 }
 
 // ---------------------------------------------------------------------------
-// Monte Carlo tiles: 32 codeword rows x kMcSamplesPerTile samples each.
+// Monte Carlo tiles (shape: mc_rows_per_lane / mc_chunks in dd_jobs.h).
+//
+// The samples of a lane are independent, so the fast loops draw several Philox
+// blocks before they bin anything: the bins are bumped by volatile asm, which
+// the compiler does not move computations across, and one block at a time
+// would leave the ten-round multiply chain of each block exposed.
 // ---------------------------------------------------------------------------
+constexpr int kMcBlocksPerStep = 4;
+
+// Many samples per codeword: one codeword per lane, up to kMcSamplesPerTile of
+// its samples, drawn kMcBlocksPerStep Philox blocks at a time.
 template <int kMode>
-__device__ void mc_tile(const Job& J, uint64_t lt, uint32_t* wbins, int lane, unsigned* status) {
-  const uint64_t chunks = (J.iters - J.sample_begin + kMcSamplesPerTile - 1) / kMcSamplesPerTile;
-  const uint64_t rt = lt / chunks, ch = lt % chunks;
-  const uint64_t i = rt * 32 + lane;
-  if (i >= J.rows) return;
-  const uint64_t t0 = J.sample_begin + ch * kMcSamplesPerTile;
-  const uint64_t t1 = t0 + kMcSamplesPerTile < J.iters ? t0 + kMcSamplesPerTile : J.iters;
-  const uint32_t lane_base = (uint32_t)__cvta_generic_to_shared(wbins) + (uint32_t)lane * 4u;
+__device__ __forceinline__ void mc_many(const Job& J, uint64_t i, uint64_t t, uint64_t t1, uint32_t lane_base,
+                                        unsigned* status) {
   const uint64_t w = J.A * i;
   const uint32_t k0 = (uint32_t)J.seed, k1 = (uint32_t)(J.seed >> 32);
   const uint32_t i0 = (uint32_t)i, i1 = (uint32_t)(i >> 32);
   if (J.n <= 32) {
+    // four 32-bit samples per block (counter (t >> 2, i)); index = top n bits
     const unsigned sh = 32 - J.n;
-    const uint32_t wl = (uint32_t)w, wh = (uint32_t)(w >> 32);
-    const uint32_t a = (uint32_t)J.A;
-    uint64_t t = t0;
-    // up to the next Philox block boundary (t0 is not a multiple of 4 when a
-    // continued run starts inside a block)
+    const uint32_t wl = (uint32_t)w;
+    const uint32_t a = (uint32_t)J.A;  // A < 2^32
+    const bool wide = J.wide != 0;
+    // up to the next block boundary (a continued run may start inside a block)
     for (; t < t1 && (t & 3); ++t) {
       const uint64_t v = J.A * mc_index(J.seed, i, t, J.n);
       bump_checked<kMode>(lane_base, popc64(w ^ v), J.nbins, status);
     }
-    // whole Philox blocks
-    for (; t + 4 <= t1; t += 4) {
-      const uint64_t blk = t >> 2;
-      const Philox4 o = philox4x32_10((uint32_t)blk, (uint32_t)(blk >> 32), i0, i1, k0, k1);
-      const uint32_t r[4] = {o.x, o.y, o.z, o.w};
+    constexpr int kS = 4 * kMcBlocksPerStep;
+    for (; t + kS <= t1; t += kS) {
+      uint32_t r[kS], d[kS];
 #pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        const uint32_t jj = sh == 32 ? 0u : (r[u] >> sh);
-        if (J.wide || (J.A >> 32)) {
-          const uint64_t v = J.A * (uint64_t)jj;
-          bump_checked<kMode>(lane_base, popc64(w ^ v), J.nbins, status);
-        } else {
-          bump_checked<kMode>(lane_base, __popc(wl ^ (a * jj)), J.nbins, status);
-        }
+      for (int b = 0; b < kMcBlocksPerStep; ++b) {
+        const uint64_t blk = (t >> 2) + b;
+        const Philox4 o = philox4x32_10((uint32_t)blk, (uint32_t)(blk >> 32), i0, i1, k0, k1);
+        r[4 * b] = o.x; r[4 * b + 1] = o.y; r[4 * b + 2] = o.z; r[4 * b + 3] = o.w;
       }
-    }
-    (void)wh;
-    for (; t < t1; ++t) {
-      const uint64_t v = J.A * mc_index(J.seed, i, t, J.n);
-      bump_checked<kMode>(lane_base, popc64(w ^ v), J.nbins, status);
+      if (wide) {
+#pragma unroll
+        for (int u = 0; u < kS; ++u) d[u] = popc64(w ^ ((uint64_t)a * (r[u] >> sh)));
+      } else {
+#pragma unroll
+        for (int u = 0; u < kS; ++u) d[u] = __popc(wl ^ (a * (r[u] >> sh)));
+      }
+#pragma unroll
+      for (int u = 0; u < kS; ++u) bump_checked<kMode>(lane_base, d[u], J.nbins, status);
     }
   } else {
-    for (uint64_t t = t0; t < t1; ++t) {
+    // two 64-bit samples per block (counter (t >> 1, i)); index = top n bits
+    const unsigned sh = 64 - J.n;
+    if (t < t1 && (t & 1)) {
       const uint64_t v = J.A * mc_index(J.seed, i, t, J.n);
       bump_checked<kMode>(lane_base, popc64(w ^ v), J.nbins, status);
+      ++t;
     }
+    constexpr int kS = 2 * kMcBlocksPerStep;
+    for (; t + kS <= t1; t += kS) {
+      uint64_t r[kS];
+      uint32_t d[kS];
+#pragma unroll
+      for (int b = 0; b < kMcBlocksPerStep; ++b) {
+        const uint64_t blk = (t >> 1) + b;
+        const Philox4 o = philox4x32_10((uint32_t)blk, (uint32_t)(blk >> 32), i0, i1, k0, k1);
+        r[2 * b] = ((uint64_t)o.x << 32) | o.y;
+        r[2 * b + 1] = ((uint64_t)o.z << 32) | o.w;
+      }
+#pragma unroll
+      for (int u = 0; u < kS; ++u) d[u] = popc64(w ^ ((uint64_t)(uint32_t)J.A * (r[u] >> sh)));
+#pragma unroll
+      for (int u = 0; u < kS; ++u) bump_checked<kMode>(lane_base, d[u], J.nbins, status);
+    }
+  }
+  for (; t < t1; ++t) {
+    const uint64_t v = J.A * mc_index(J.seed, i, t, J.n);
+    bump_checked<kMode>(lane_base, popc64(w ^ v), J.nbins, status);
+  }
+}
+
+// Few samples per codeword (fewer than kMcSamplesPerTile): each lane takes
+// several codewords with all of their samples, one Philox block at a time.
+template <int kMode>
+__device__ __noinline__ void mc_few(uint64_t A, uint64_t seed, uint32_t n, uint32_t nbins, uint64_t i, uint64_t t,
+                                    uint64_t t1, uint32_t lane_base, unsigned* status) {
+  const uint64_t w = A * i;
+  const uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32);
+  const uint32_t i0 = (uint32_t)i, i1 = (uint32_t)(i >> 32);
+  const uint64_t a = (uint32_t)A;  // A < 2^32
+  const unsigned per_block = n <= 32 ? 4u : 2u;
+  for (; t < t1 && (t & (per_block - 1)); ++t)
+    bump_checked<kMode>(lane_base, popc64(w ^ (A * mc_index(seed, i, t, n))), nbins, status);
+  for (; t + per_block <= t1; t += per_block) {
+    const uint64_t blk = t / per_block;
+    const Philox4 o = philox4x32_10((uint32_t)blk, (uint32_t)(blk >> 32), i0, i1, k0, k1);
+    if (per_block == 4) {
+      const unsigned sh = 32 - n;
+      const uint32_t d0 = popc64(w ^ (a * (o.x >> sh))), d1 = popc64(w ^ (a * (o.y >> sh)));
+      const uint32_t d2 = popc64(w ^ (a * (o.z >> sh))), d3 = popc64(w ^ (a * (o.w >> sh)));
+      bump_checked<kMode>(lane_base, d0, nbins, status);
+      bump_checked<kMode>(lane_base, d1, nbins, status);
+      bump_checked<kMode>(lane_base, d2, nbins, status);
+      bump_checked<kMode>(lane_base, d3, nbins, status);
+    } else {
+      const unsigned sh = 64 - n;
+      const uint32_t d0 = popc64(w ^ (a * ((((uint64_t)o.x << 32) | o.y) >> sh)));
+      const uint32_t d1 = popc64(w ^ (a * ((((uint64_t)o.z << 32) | o.w) >> sh)));
+      bump_checked<kMode>(lane_base, d0, nbins, status);
+      bump_checked<kMode>(lane_base, d1, nbins, status);
+    }
+  }
+  for (; t < t1; ++t) bump_checked<kMode>(lane_base, popc64(w ^ (A * mc_index(seed, i, t, n))), nbins, status);
+}
+
+template <int kMode>
+__device__ void mc_tile(const Job& J, uint64_t lt, uint32_t* wbins, int lane, unsigned* status) {
+  const uint64_t spl = J.iters - J.sample_begin;
+  const uint64_t rpl = mc_rows_per_lane(spl), chunks = mc_chunks(spl);
+  const uint64_t rt = lt / chunks, ch = lt % chunks;
+  const uint64_t t0 = J.sample_begin + ch * kMcSamplesPerTile;
+  const uint64_t t1 = t0 + kMcSamplesPerTile < J.iters ? t0 + kMcSamplesPerTile : J.iters;
+  const uint32_t lane_base = (uint32_t)__cvta_generic_to_shared(wbins) + (uint32_t)lane * 4u;
+  if (rpl == 1) {
+    const uint64_t i = rt * 32 + lane;
+    if (i < J.rows) mc_many<kMode>(J, i, t0, t1, lane_base, status);
+    return;
+  }
+  for (uint64_t r = 0; r < rpl; ++r) {
+    const uint64_t i = (rt * rpl + r) * 32 + lane;
+    if (i >= J.rows) return;
+    mc_few<kMode>(J.A, J.seed, J.n, J.nbins, i, t0, t1, lane_base, status);
   }
 }
 

@@ -188,7 +188,10 @@ uint64_t job_tiles(const Job& j) {
       if (j.shape == SHAPE_TRIANGLE) return j.col_tiles * (j.col_tiles + 1) / 2 * kStrips;
       return ((j.rows + kWarpRows - 1) / kWarpRows) * j.col_tiles;
     case JOB_MC:
-      return ((j.rows + 31) / 32) * ((j.iters - j.sample_begin + kMcSamplesPerTile - 1) / kMcSamplesPerTile);
+    {
+      const uint64_t spl = j.iters - j.sample_begin, per_tile = 32 * mc_rows_per_lane(spl);
+      return spl ? ((j.rows + per_tile - 1) / per_tile) * mc_chunks(spl) : 0;
+    }
     default:
       return (j.iters + 32 * 256 - 1) / (32 * 256);
   }

@@ -11,13 +11,22 @@
 //
 // Work unit: the popc kernel's tile space (1024x1024 super tiles of the i<j
 // triangle, split into 8 strips of 128 rows).  A strip is 128 rows (UMMA M) x
-// 1024 columns = 4 MMA tiles of N = 256, accumulated in two TMEM buffers of 256
-// columns so that the MMA of tile t+1 overlaps the epilogue of tile t.
-// One CTA per SM (256 threads, 512 TMEM columns); operands are generated by
-// the CTA itself into shared memory in the no-swizzle K-major UMMA layout.
+// 1024 columns = 8 MMA tiles of N = 128, accumulated in four TMEM buffers of 128
+// columns, so the epilogue may trail the MMAs by three tiles before the issuer
+// has to wait for it.  Generator warps claim 8 strips at a time (one super tile
+// when the job's tile range is aligned), so the column operand of a super tile
+// is written once for its 8 strips; the row operand is double-buffered by strip
+// and written while the previous strip's MMAs run.
+// One CTA per SM (16 epilogue warps, 1 issuer warp, 3 generator warps, 512 TMEM
+// columns).
+//
+// The epilogue is bound by the shared-memory atomic rate (one red.shared per
+// pair; about 32 per clock per SM measured on B200 for TMEM-resident values),
+// twice the POPC issue rate (16 per clock per SM) that bounds the popc kernel.
 //
 // Every mbarrier wait is bounded (MmaArgs::timeout_ns); on expiry the CTA
-// records KSTATUS_TIMEOUT, releases its TMEM and returns.
+// records KSTATUS_TIMEOUT, every other wait gives up, the last MMA drains
+// (bounded) and the TMEM is released.
 #include <cuda_runtime.h>
 #include <cstdint>
 
@@ -29,18 +38,27 @@ namespace dd {
 
 namespace {
 
-constexpr int kThreads = 256;
+constexpr int kEpiWarps = 16;                          // epilogue warps
+constexpr int kEpiThreads = kEpiWarps * 32;            // 512: bin columns per bin row
+constexpr int kIssuerWarp = kEpiWarps;                 // warp 16: its lane 0 issues every MMA
+constexpr int kGenWarps = 3;                           // warps 17..19: claim, decode, write operands
+constexpr int kGenThreads = kGenWarps * 32;
+constexpr int kThreads = kEpiThreads + 32 + kGenThreads;
 constexpr int kM = 128;                 // rows per strip (UMMA M)
-constexpr int kN = 256;                 // columns per MMA tile (UMMA N)
-constexpr int kTilesPerStrip = kSuper / kN;  // 4
+constexpr int kN = 128;                 // columns per MMA tile (UMMA N)
+constexpr int kTilesPerStrip = kSuper / kN;  // 8
 constexpr int kK = 64;                  // bytes of K per row/column
 constexpr int kLBO = 128;               // bytes between K-adjacent 8x16B core matrices
 constexpr int kSBO = 512;               // bytes between M/N-adjacent 8-row groups (4 core matrices)
 constexpr int kABytes = kM * kK;        // 8 KB
-constexpr int kBTileBytes = kN * kK;    // 16 KB
+constexpr int kBTileBytes = kN * kK;    // 8 KB
 constexpr int kBBytes = kTilesPerStrip * kBTileBytes;  // 64 KB
 constexpr uint32_t kTmemCols = 512;
 constexpr uint32_t kMinSmem = 120 * 1024;  // more than half an SM: one CTA (and one TMEM owner) per SM
+constexpr int kBufs = kTmemCols / kN;   // 4 accumulator buffers
+constexpr int kColsPerWarp = kN / (kEpiWarps / 4);  // 32: each epilogue warp reads one 32-column load per tile
+static_assert(kEpiWarps % 4 == 0 && kColsPerWarp == 32, "one 32-column TMEM load per warp and tile");
+static_assert(kBufs == 4, "buffer index and phase arithmetic below assume 4 buffers");
 
 // ---------------------------------------------------------------- PTX wrappers
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -102,7 +120,7 @@ __device__ __forceinline__ uint64_t smem_desc(uint32_t addr) {
   return d;  // base offset 0, absolute-LBO mode off, layout type 0 (SWIZZLE_NONE)
 }
 
-// Instruction descriptor: D = S32, A = B = signed 8-bit, both K-major, M=128, N=256.
+// Instruction descriptor: D = S32, A = B = signed 8-bit, both K-major, M=128, N=128.
 constexpr uint32_t kIdesc = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(kN >> 3) << 17) |
                             ((uint32_t)(kM >> 4) << 24);
 
@@ -120,7 +138,8 @@ __device__ __forceinline__ void mma_commit(uint32_t mbar) {
                : "memory");
 }
 
-__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
+// 32 consecutive TMEM columns of this warp's 32 lanes; tmem_wait_ld completes it.
+__device__ __forceinline__ void tmem_ld32_nowait(uint32_t taddr, uint32_t (&v)[32]) {
   asm volatile(
       "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
       "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
@@ -130,8 +149,8 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
         "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]),
         "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
       : "r"(taddr));
-  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
 __device__ __forceinline__ void red_shared(uint32_t addr) {
   asm volatile("red.shared.add.u32 [%0], 1;" ::"r"(addr) : "memory");
@@ -190,176 +209,313 @@ __device__ __forceinline__ uint32_t find_job(const Job* jobs, uint32_t njobs, ui
   return lo;
 }
 
-struct Shared {
-  uint64_t mbar[2];
-  uint32_t tmem_base;
-  uint32_t flag;
-  unsigned long long item;
+// One TMEM buffer's tile, published by the issuer with its MMA.
+struct TileInfo {
+  unsigned long long r0;  // first row (codeword index) of the strip
+  unsigned long long c0;  // first column of this N = 128 tile
+  unsigned long long n;   // codewords of the job
+  uint32_t job;           // job index
+  uint32_t flags;         // kInfoDone | kInfoFull
 };
+constexpr uint32_t kInfoDone = 1u, kInfoFull = 2u;
+
+// One strip (128 rows x one super tile of columns) as the generators publish it.
+struct StripInfo {
+  unsigned long long r0, c0, n;
+  uint32_t job, flags;  // kInfoDone | kInfoFull
+};
+
+struct Shared {
+  uint64_t full[kBufs];   // tile in TMEM buffer b ready: tcgen05.commit + the issuer's arrive (count 2)
+  uint64_t empty[kBufs];  // TMEM buffer b read: one arrive per epilogue warp (count kEpiWarps)
+  TileInfo info[kBufs];
+  // strip queue, generators -> issuer (slot = strip & 1, with that slot's row operand)
+  StripInfo strip[2];
+  uint64_t slot_full[2];  // strip ready: the generators' thread 0 arrives (count 1)
+  uint64_t slot_free[2];  // every MMA of the strip done: tcgen05.commit after its last tile (count 1)
+  uint32_t tmem_base;
+  uint32_t abort;         // set by whichever wait ran out; every other wait then gives up too
+  uint32_t gflag;         // generators: result of their thread 0's wait
+  uint32_t pad;
+  unsigned long long gclaim;  // generators: first strip of the current claim
+};
+
+// Barrier 1 over the generator warps only (barrier 0 is __syncthreads).
+__device__ __forceinline__ void gen_bar() { asm volatile("bar.sync 1, %0;" ::"n"(kGenThreads) : "memory"); }
+
+__device__ __forceinline__ void mbar_arrive(uint32_t addr) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(addr) : "memory");
+}
+
+// Bounded wait (single thread): true when the phase completed; false after
+// timeout_ns or once another thread has aborted (then this one aborts too).
+__device__ __forceinline__ bool wait_or_abort(uint32_t addr, uint32_t parity, unsigned long long timeout_ns,
+                                              volatile uint32_t* abort) {
+  if (mbar_try_wait(addr, parity)) return true;
+  const uint64_t t0 = globaltimer();
+  while (true) {
+    if (mbar_try_wait(addr, parity)) return true;
+    if (*abort) return false;
+    if (globaltimer() - t0 > timeout_ns) {
+      *abort = 1u;
+      return false;
+    }
+  }
+}
 
 }  // namespace
 
 // ---------------------------------------------------------------- kernel
+// Warp roles: warps 0..15 bin (epilogue), warp 16 issues the MMAs (lane 0),
+// warps 17..19 claim strips and write their operands.  Hand-offs go through
+// mbarriers only: slot_full/slot_free (a strip's operands written / its MMAs
+// done), full[b] (the MMA result in TMEM buffer b and its TileInfo are ready),
+// empty[b] (all 16 epilogue warps have read buffer b).  No CTA-wide barrier
+// runs between set-up and exit.
+//
+// Epilogue warp w reads TMEM lanes 32*(w%4).. (its rows) and 32 columns
+// 32*(w/4).. of each 128-column tile, and bumps one shared-memory counter per
+// pair in its own bin columns (row stride kEpiThreads words), so warps never
+// share a counter and each warp flushes its own columns.
 __global__ void __launch_bounds__(kThreads, 1) mma_hist_kernel(MmaArgs args) {
   extern __shared__ __align__(1024) uint8_t smem[];
-  uint8_t* sA = smem;                                    // 8 KB
-  uint8_t* sB = smem + kABytes;                          // 64 KB
-  uint32_t* hist = reinterpret_cast<uint32_t*>(smem + kABytes + kBBytes);  // hist_rows x 256
-  Shared* sh = reinterpret_cast<Shared*>(smem + kABytes + kBBytes + (size_t)args.hist_rows * kThreads * 4);
+  uint8_t* sB = smem;                                        // 64 KB: 8 column tiles of one super tile
+  uint8_t* sA = smem + kBBytes;                              // 2 x 8 KB: row operand, double-buffered by strip
+  uint32_t* hist = reinterpret_cast<uint32_t*>(smem + kBBytes + 2 * kABytes);  // hist_rows x kEpiThreads
+  Shared* sh = reinterpret_cast<Shared*>(smem + kBBytes + 2 * kABytes + (size_t)args.hist_rows * kEpiThreads * 4);
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int wg = warp >> 2, q = warp & 3;  // warpgroup (column half) and TMEM lane quarter
-  const uint32_t trash = args.hist_rows - 1;
+  volatile uint32_t* abort = &sh->abort;
 
-  for (uint32_t k = tid; k < args.hist_rows * kThreads; k += kThreads) hist[k] = 0;
+  for (uint32_t k = tid; k < args.hist_rows * kEpiThreads; k += kThreads) hist[k] = 0;
   if (tid == 0) {
-    mbar_init(smem_u32(&sh->mbar[0]), 1);
-    mbar_init(smem_u32(&sh->mbar[1]), 1);
+    for (int b = 0; b < kBufs; ++b) {
+      mbar_init(smem_u32(&sh->full[b]), 2);
+      mbar_init(smem_u32(&sh->empty[b]), kEpiWarps);
+    }
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(smem_u32(&sh->slot_full[b]), 1);
+      mbar_init(smem_u32(&sh->slot_free[b]), 1);
+    }
+    sh->abort = 0;
     fence_mbar_init();
   }
-  if (warp == 0) tmem_alloc(smem_u32(&sh->tmem_base), kTmemCols);
-  // The K-padding chunk (bytes 48..63) is zero for every operand with L <= 44;
-  // write_operand rewrites all four chunks, so nothing relies on this.
+  if (warp == kIssuerWarp) tmem_alloc(smem_u32(&sh->tmem_base), kTmemCols);
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = sh->tmem_base;
-  const uint32_t hist_lane = smem_u32(hist) + (uint32_t)tid * 4u;
 
-  uint32_t phase0 = 0, phase1 = 0;  // used by thread 0 only
-  uint32_t cur = 0xffffffffu, since_flush = 0;
-  bool failed = false;
-  Job J;
-
-  auto flush = [&](const Job& job) {
-    __syncthreads();
-    for (uint32_t b = tid; b < args.hist_rows; b += kThreads) {
-      unsigned long long s = 0;
-      for (int k = 0; k < kThreads; ++k) {
-        const int kk = (k + tid) & (kThreads - 1);
-        s += hist[b * kThreads + kk];
-        hist[b * kThreads + kk] = 0;
+  if (warp > kIssuerWarp) {
+    // ------------------------------------------------------------ generators
+    // All kGenThreads threads walk the same strips (uniform control flow
+    // between the named barriers); their thread 0 claims work and waits.
+    const int gtid = tid - (kEpiThreads + 32);
+    uint64_t s = 0;  // strips published
+    uint32_t bjob = 0xffffffffu;
+    uint64_t bsc = ~0ull;  // column super tile whose operand is in sB
+    unsigned long long t = 0, end = 0;
+    bool normal = false;
+    for (;;) {
+      if (t >= end) {
+        if (gtid == 0) sh->gclaim = atomicAdd(args.counter, (unsigned long long)kStrips);
+        gen_bar();
+        const unsigned long long base = sh->gclaim;
+        if (base >= args.total_tiles) { normal = true; break; }
+        t = base;
+        end = base + kStrips < args.total_tiles ? base + (unsigned long long)kStrips
+                                                : (unsigned long long)args.total_tiles;
       }
-      if (b == trash) {
-        if (s) atomicOr(args.status, KSTATUS_BAD_DISTANCE);
-      } else if (s && b < job.nbins) {
-        atomicAdd(job.bins + b, s);
-      } else if (s) {
-        atomicOr(args.status, KSTATUS_BAD_DISTANCE);
+      const unsigned long long tt = t++;
+      const uint32_t jn = find_job(args.jobs, args.njobs, tt);
+      if (jn >= args.njobs) {
+        if (gtid == 0) atomicOr(args.status, KSTATUS_BAD_JOB);
+        continue;
       }
-    }
-    __syncthreads();
-  };
-
-  while (true) {
-    if (tid == 0) sh->item = atomicAdd(args.counter, 1ull);
-    __syncthreads();
-    const unsigned long long t = sh->item;
-    __syncthreads();
-    if (t >= args.total_tiles) break;
-    const uint32_t jn = find_job(args.jobs, args.njobs, t);
-    if (jn != cur) {
-      if (cur != 0xffffffffu && since_flush) flush(J);
-      since_flush = 0;
-      J = args.jobs[jn];
-      cur = jn;
-    }
-    const uint64_t lt = t - J.tile_begin + J.tile_offset;
-    uint64_t sr, sc;
-    tri_decode(lt / kStrips, J.col_tiles, sr, sc);
-    const uint64_t r0 = sr * kSuper + (lt % kStrips) * kM;
-    const uint64_t c0 = sc * kSuper;
-    const uint64_t N = J.rows;
-    const bool full = (r0 + kM <= N) && (c0 + kSuper <= N) && sr != sc;
-    if (r0 >= N) continue;  // CTA-uniform: every thread saw the same item
-
-    // operand bit planes: L = bits of the largest codeword, rounded up to 4
-    const uint64_t maxcw = J.A * (N - 1);
-    int L = 64 - __clzll((long long)(maxcw | 1));
-    L = (L + 3) & ~3;
-
-    // ---- operands: rows (A) by threads 0..127, 1024 columns (B) by all
-    if (tid < kM) {
-      const uint64_t i = r0 + tid;
-      write_operand(sA, tid, i < N ? J.A * i : 0, L, true);
-    }
+      const Job* jp = args.jobs + jn;
+      const uint64_t tb = __ldg(&jp->tile_begin), tiles = __ldg(&jp->tiles);
+      if (tt < tb || tt - tb >= tiles) {
+        if (gtid == 0) atomicOr(args.status, KSTATUS_BAD_JOB);
+        continue;
+      }
+      const uint64_t A = __ldg(&jp->A), N = __ldg(&jp->rows);
+      const uint64_t lt = tt - tb + __ldg(&jp->tile_offset);
+      uint64_t sr, sc;
+      tri_decode(lt / kStrips, __ldg(&jp->col_tiles), sr, sc);
+      const uint64_t r0 = sr * kSuper + (lt % kStrips) * kM;
+      const uint64_t c0 = sc * kSuper;
+      if (r0 >= N) continue;  // uniform over the group
+      const bool full = (r0 + kM <= N) && (c0 + kSuper <= N) && sr != sc;
+      const uint64_t maxcw = A * (N - 1);
+      int L = 64 - __clzll((long long)(maxcw | 1));
+      L = (L + 3) & ~3;
+      const uint32_t slot = (uint32_t)(s & 1);
+      const bool need_b = jn != bjob || sc != bsc;
+      // the column operand may be rewritten once every MMA of strip s-1 is done,
+      // this slot's row operand once every MMA of strip s-2 is done
+      if (gtid == 0) {
+        bool ok = true;
+        if (need_b && s >= 1)
+          ok = wait_or_abort(smem_u32(&sh->slot_free[(s - 1) & 1]), (uint32_t)((s - 1) >> 1) & 1u, args.timeout_ns,
+                             abort);
+        else if (s >= 2)
+          ok = wait_or_abort(smem_u32(&sh->slot_free[slot]), (uint32_t)((s - 2) >> 1) & 1u, args.timeout_ns, abort);
+        sh->gflag = ok ? 1u : 0u;
+      }
+      gen_bar();
+      if (!sh->gflag) break;
+      if (need_b) {
 #pragma unroll 1
-    for (int cc = tid; cc < kSuper; cc += kThreads) {
-      const uint64_t j = c0 + cc;
-      write_operand(sB + (cc / kN) * kBTileBytes, cc % kN, j < N ? J.A * j : 0, L, false);
-    }
-    fence_proxy_async();
-    __syncthreads();
-
-    const uint32_t mbar0 = smem_u32(&sh->mbar[0]), mbar1 = smem_u32(&sh->mbar[1]);
-    auto issue = [&](int tile) {
-      const uint32_t d = tmem + (uint32_t)(tile & 1) * kN;
-      const uint32_t a0 = smem_u32(sA), b0 = smem_u32(sB + tile * kBTileBytes);
-#pragma unroll
-      for (int ks = 0; ks < kK / 32; ++ks)  // K = 32 bytes per instruction = 2 core matrices
-        mma_i8(d, smem_desc(a0 + ks * 2 * kLBO), smem_desc(b0 + ks * 2 * kLBO), ks > 0 ? 1u : 0u);
-      mma_commit((tile & 1) ? mbar1 : mbar0);
-    };
-    if (tid == 0) {
-      tc_fence_after();
-      issue(0);
-      issue(1);
-    }
-
-    for (int tile = 0; tile < kTilesPerStrip; ++tile) {
-      const int b = tile & 1;
-      if (tid == 0) {
-        const bool ok = mbar_wait_bounded(b ? mbar1 : mbar0, b ? phase1 : phase0, args.timeout_ns);
-        if (b) phase1 ^= 1; else phase0 ^= 1;
-        sh->flag = ok ? 1u : 0u;
+        for (int cc = gtid; cc < kSuper; cc += kGenThreads) {
+          const uint64_t j = c0 + cc;
+          write_operand(sB + (cc / kN) * kBTileBytes, cc % kN, j < N ? A * j : 0, L, false);
+        }
+        bjob = jn;
+        bsc = sc;
       }
-      __syncthreads();
-      if (!sh->flag) { failed = true; break; }
-      tc_fence_after();
-      // ---- epilogue: this thread's TMEM lane (row) x 128 columns of the tile
-      const uint32_t row = (uint32_t)(q * 32 + lane);
-      const uint64_t i = r0 + row;
-      const uint64_t jbase = c0 + (uint64_t)tile * kN + (uint64_t)wg * 128;
+      uint8_t* a = sA + slot * kABytes;
 #pragma unroll 1
-      for (int cc = 0; cc < 4; ++cc) {
-        uint32_t v[32];
-        __syncwarp();  // tcgen05.ld is warp-collective: reconverge after the masked branch
-        tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)b * kN + (uint32_t)wg * 128 + cc * 32, v);
-        if (full) {
+      for (int rr = gtid; rr < kM; rr += kGenThreads) {
+        const uint64_t i = r0 + rr;
+        write_operand(a, rr, i < N ? A * i : 0, L, true);
+      }
+      fence_proxy_async();
+      gen_bar();  // both operands complete
+      if (gtid == 0) {
+        StripInfo& si = sh->strip[slot];
+        si.r0 = r0;
+        si.c0 = c0;
+        si.n = N;
+        si.job = jn;
+        si.flags = full ? kInfoFull : 0u;
+        mbar_arrive(smem_u32(&sh->slot_full[slot]));
+      }
+      ++s;
+    }
+    if (gtid == 0 && normal) {
+      // the issuer has finished with strip s-2 (this slot) once that strip's MMAs are done
+      if (s < 2 || wait_or_abort(smem_u32(&sh->slot_free[s & 1]), (uint32_t)((s - 2) >> 1) & 1u, args.timeout_ns,
+                                 abort)) {
+        sh->strip[s & 1].flags = kInfoDone;
+        mbar_arrive(smem_u32(&sh->slot_full[s & 1]));
+      }
+    }
+  } else if (warp == kIssuerWarp) {
+    // ------------------------------------------------------------ issuer (lane 0)
+    if (lane == 0) {
+      uint64_t g = 0;  // tiles issued
+      bool normal = false;
+      // until the epilogue has read tile gg-4, the previous tile of gg's buffer
+      auto wait_empty = [&](uint64_t gg) -> bool {
+        return gg < kBufs ||
+               wait_or_abort(smem_u32(&sh->empty[gg & 3]), (uint32_t)((gg - kBufs) >> 2) & 1u, args.timeout_ns, abort);
+      };
+      for (uint64_t s = 0;; ++s) {
+        const uint32_t slot = (uint32_t)(s & 1);
+        if (!wait_or_abort(smem_u32(&sh->slot_full[slot]), (uint32_t)(s >> 1) & 1u, args.timeout_ns, abort)) break;
+        const StripInfo si = sh->strip[slot];
+        if (si.flags & kInfoDone) { normal = true; break; }
+        const uint32_t a0 = smem_u32(sA + slot * kABytes);
+        bool ok = true;
+        for (int tile = 0; tile < kTilesPerStrip; ++tile, ++g) {
+          if (!wait_empty(g)) { ok = false; break; }
+          const uint32_t b = (uint32_t)(g & 3);
+          TileInfo& ti = sh->info[b];
+          ti.r0 = si.r0;
+          ti.c0 = si.c0 + (uint64_t)tile * kN;
+          ti.n = si.n;
+          ti.job = si.job;
+          ti.flags = si.flags & kInfoFull;
+          tc_fence_after();
+          const uint32_t d = tmem + b * (uint32_t)kN;
+          const uint32_t b0 = smem_u32(sB + tile * kBTileBytes);
 #pragma unroll
-          for (int u = 0; u < 32; ++u) red_shared(hist_lane + (min(v[u], trash) << 10));
-        } else {
-#pragma unroll
-          for (int u = 0; u < 32; ++u) {
-            const uint64_t j = jbase + cc * 32 + u;
-            if (i < N && j < N && j > i) red_shared(hist_lane + (min(v[u], trash) << 10));
-          }
+          for (int ks = 0; ks < kK / 32; ++ks)  // K = 32 bytes per instruction = 2 core matrices
+            mma_i8(d, smem_desc(a0 + ks * 2 * kLBO), smem_desc(b0 + ks * 2 * kLBO), ks > 0 ? 1u : 0u);
+          mma_commit(smem_u32(&sh->full[b]));
+          mbar_arrive(smem_u32(&sh->full[b]));
+        }
+        if (!ok) break;
+        mma_commit(smem_u32(&sh->slot_free[slot]));  // the strip's operands are free once its MMAs are done
+      }
+      if (normal && wait_empty(g)) {
+        // end of work: a tile marked done wakes the epilogue warps
+        sh->info[g & 3].flags = kInfoDone;
+        mbar_arrive(smem_u32(&sh->full[g & 3]));
+        mbar_arrive(smem_u32(&sh->full[g & 3]));
+      } else {
+        *abort = 1u;
+        atomicOr(args.status, KSTATUS_TIMEOUT);
+        // let the last MMA drain (bounded, in-order completion) before TMEM is released
+        if (g > 0) mbar_wait_bounded(smem_u32(&sh->full[(g - 1) & 3]), (uint32_t)((g - 1) >> 2) & 1u, args.timeout_ns);
+      }
+    }
+    __syncwarp();
+  } else {
+    // ------------------------------------------------------------ epilogue
+    const int q = warp & 3, sub = warp >> 2;
+    const uint32_t hist_lane = smem_u32(hist) + (uint32_t)tid * 4u;
+    const uint32_t trash = args.hist_rows - 1;  // distances the bins cannot hold land here (flagged at flush)
+    uint32_t cur = 0xffffffffu, nbins = 0, since_flush = 0;
+    unsigned long long* bins = nullptr;
+    bool ok = true;
+    // this warp's bin columns -> the job's global bins
+    auto flush = [&]() {
+      for (uint32_t b = 0; b < args.hist_rows; ++b) {
+        const uint32_t x = hist[b * kEpiThreads + tid];
+        hist[b * kEpiThreads + tid] = 0;
+        const uint32_t s = __reduce_add_sync(0xffffffffu, x);
+        if (lane == 0 && s) {
+          if (b < nbins) atomicAdd(bins + b, (unsigned long long)s);
+          else atomicOr(args.status, KSTATUS_BAD_DISTANCE);
         }
       }
+    };
+    for (uint64_t g = 0;; ++g) {
+      const uint32_t b = (uint32_t)(g & 3);
+      bool r = true;
+      if (lane == 0) r = wait_or_abort(smem_u32(&sh->full[b]), (uint32_t)(g >> 2) & 1u, args.timeout_ns, abort);
+      if (!__shfl_sync(0xffffffffu, r ? 1 : 0, 0)) { ok = false; break; }
+      __syncwarp();  // lane 0's wait acquired the issuer's TileInfo; this orders it for the warp
+      const TileInfo& ti = sh->info[b];
+      const uint32_t flags = ti.flags;
+      if (flags & kInfoDone) break;
+      const uint32_t job = ti.job;
+      tc_fence_after();
+      uint32_t v[32];
+      tmem_ld32_nowait(tmem + ((uint32_t)(q * 32) << 16) + b * (uint32_t)kN + (uint32_t)(sub * kColsPerWarp), v);
+      const unsigned long long r0 = ti.r0, c0 = ti.c0, n = ti.n;
+      tmem_wait_ld();
+      // the buffer may be refilled as soon as every warp has its values in registers
       tc_fence_before();
-      __syncthreads();
-      if (tid == 0 && tile + 2 < kTilesPerStrip) {
-        tc_fence_after();
-        issue(tile + 2);
+      __syncwarp();
+      if (lane == 0) mbar_arrive(smem_u32(&sh->empty[b]));
+      if (job != cur) {
+        if (cur != 0xffffffffu && since_flush) flush();
+        since_flush = 0;
+        cur = job;
+        bins = args.jobs[job].bins;
+        nbins = args.jobs[job].nbins;
       }
+      if (flags & kInfoFull) {
+#pragma unroll
+        for (int u = 0; u < 32; ++u) red_shared(hist_lane + (min(v[u], trash) << 11));
+      } else {
+        const uint64_t i = r0 + (uint64_t)(q * 32 + lane);
+        const uint64_t j0 = c0 + (uint64_t)(sub * kColsPerWarp);
+#pragma unroll
+        for (int u = 0; u < 32; ++u) {
+          const uint64_t j = j0 + u;
+          if (i < n && j < n && j > i) red_shared(hist_lane + (min(v[u], trash) << 11));
+        }
+      }
+      if (++since_flush >= kFlushEvery) { flush(); since_flush = 0; }
     }
-    if (failed) break;
-    if (++since_flush >= kFlushEvery) { flush(J); since_flush = 0; }
-  }
-  if (failed) {
-    if (tid == 0) atomicOr(args.status, KSTATUS_TIMEOUT);
-    // let any MMA still in flight drain (bounded) before TMEM is released
-    if (tid == 0) {
-      mbar_wait_bounded(smem_u32(&sh->mbar[0]), phase0, args.timeout_ns);
-      mbar_wait_bounded(smem_u32(&sh->mbar[1]), phase1, args.timeout_ns);
-    }
-    __syncthreads();
-  } else if (cur != 0xffffffffu && since_flush) {
-    flush(J);
+    if (ok && cur != 0xffffffffu && since_flush) flush();
   }
   tc_fence_before();
   __syncthreads();
-  if (warp == 0) {
+  if (warp == kIssuerWarp) {
     tc_fence_after();
     tmem_dealloc(tmem, kTmemCols);
   }
@@ -377,7 +533,7 @@ bool mma_eligible(const Job& j) {
 }
 
 size_t mma_smem_bytes(uint32_t hist_rows) {
-  size_t s = (size_t)kABytes + kBBytes + (size_t)hist_rows * kThreads * 4 + sizeof(Shared) + 64;
+  size_t s = (size_t)2 * kABytes + kBBytes + (size_t)hist_rows * kEpiThreads * 4 + sizeof(Shared) + 64;
   return s < kMinSmem ? kMinSmem : s;
 }
 

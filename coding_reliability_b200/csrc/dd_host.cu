@@ -169,7 +169,10 @@ static int plan_launch(dd_context* ctx, std::vector<Job>& jobs, const std::vecto
   }
   lp.margs.jobs = ctx->d_jobs + lp.npopc;
   lp.margs.njobs = lp.nmma;
-  lp.margs.hist_rows = maxbm + 1;  // + the row that catches out-of-range distances
+  // rows for every distance an operand can produce (<= L), flagged at flush when >= nbins
+  uint32_t maxl = 0;
+  for (uint32_t k = lp.npopc; k < table.size(); ++k) maxl = std::max(maxl, (uint32_t)mma_operand_bits(table[k]));
+  lp.margs.hist_rows = std::max(maxbm, maxl + 1);
   lp.margs.total_tiles = tm;
   lp.margs.counter = ctx->d_ctl + 1;
   lp.margs.status = status;

@@ -276,7 +276,10 @@ __device__ __forceinline__ bool wait_or_abort(uint32_t addr, uint32_t parity, un
 // Epilogue warp w reads TMEM lanes 32*(w%4).. (its rows) and 32 columns
 // 32*(w/4).. of each 128-column tile, and bumps one shared-memory counter per
 // pair in its own bin columns (row stride kEpiThreads words), so warps never
-// share a counter and each warp flushes its own columns.
+// share a counter and each warp flushes its own columns.  A distance is at
+// most L (both operands have L bit planes, popc(x) <= L), and there are at
+// least L + 1 bin rows (mma_hist_rows), so it indexes the rows unchecked;
+// rows at or above the job's bin count are flagged at the flush.
 __global__ void __launch_bounds__(kThreads, 1) mma_hist_kernel(MmaArgs args) {
   extern __shared__ __align__(1024) uint8_t smem[];
   uint8_t* sB = smem;                                        // 64 KB: 8 column tiles of one super tile
@@ -455,7 +458,6 @@ __global__ void __launch_bounds__(kThreads, 1) mma_hist_kernel(MmaArgs args) {
     // ------------------------------------------------------------ epilogue
     const int q = warp & 3, sub = warp >> 2;
     const uint32_t hist_lane = smem_u32(hist) + (uint32_t)tid * 4u;
-    const uint32_t trash = args.hist_rows - 1;  // distances the bins cannot hold land here (flagged at flush)
     uint32_t cur = 0xffffffffu, nbins = 0, since_flush = 0;
     unsigned long long* bins = nullptr;
     bool ok = true;
@@ -499,14 +501,14 @@ __global__ void __launch_bounds__(kThreads, 1) mma_hist_kernel(MmaArgs args) {
       }
       if (flags & kInfoFull) {
 #pragma unroll
-        for (int u = 0; u < 32; ++u) red_shared(hist_lane + (min(v[u], trash) << 11));
+        for (int u = 0; u < 32; ++u) red_shared(hist_lane + (v[u] << 11));
       } else {
         const uint64_t i = r0 + (uint64_t)(q * 32 + lane);
         const uint64_t j0 = c0 + (uint64_t)(sub * kColsPerWarp);
 #pragma unroll
         for (int u = 0; u < 32; ++u) {
           const uint64_t j = j0 + u;
-          if (i < n && j < n && j > i) red_shared(hist_lane + (min(v[u], trash) << 11));
+          if (i < n && j < n && j > i) red_shared(hist_lane + (v[u] << 11));
         }
       }
       if (++since_flush >= kFlushEvery) { flush(); since_flush = 0; }
@@ -522,6 +524,16 @@ __global__ void __launch_bounds__(kThreads, 1) mma_hist_kernel(MmaArgs args) {
 }
 
 // ---------------------------------------------------------------- host side
+// Bit planes of the operands of job j: the bits of its largest codeword, rounded
+// up to 4 (the kernel computes the same from the job).
+int mma_operand_bits(const Job& j) {
+  const unsigned __int128 maxcw = (unsigned __int128)j.A * (j.rows - 1);
+  int bits = 0;
+  for (unsigned __int128 v = maxcw; v; v >>= 1) ++bits;
+  if (bits == 0) bits = 1;
+  return (bits + 3) & ~3;
+}
+
 bool mma_eligible(const Job& j) {
   if (j.kind != JOB_PAIRS || j.shape != SHAPE_TRIANGLE || j.row_kind != ROW_PROGRESSION ||
       j.col_kind != COL_PROGRESSION)

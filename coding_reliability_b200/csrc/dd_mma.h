@@ -11,7 +11,7 @@ namespace dd {
 struct MmaArgs {
   const Job* jobs;
   uint32_t njobs;
-  uint32_t hist_rows;        // bin rows in shared memory (max nbins + 1 trash row)
+  uint32_t hist_rows;        // bin rows in shared memory: >= every job's nbins and operand bits + 1
   uint64_t total_tiles;      // work items: (super tile, 128-row strip) as in the popc kernel
   unsigned long long* counter;
   unsigned* status;          // KSTATUS_* bits, zeroed before the launch
@@ -20,6 +20,8 @@ struct MmaArgs {
 
 // True if the job can run on the MMA path (AN exhaustive, codewords <= 60 bits).
 bool mma_eligible(const Job& j);
+// Operand bit planes L of job j; its distances lie in [0, L].
+int mma_operand_bits(const Job& j);
 size_t mma_smem_bytes(uint32_t hist_rows);
 cudaError_t launch_mma(const MmaArgs& args, int grid, size_t smem, cudaStream_t stream);
 

@@ -169,6 +169,7 @@ def load() -> C.CDLL:
     lib.dd_philox4x32_10.argtypes = [C.POINTER(u32), C.POINTER(u32), C.POINTER(u32)]
     lib.dd_philox4x32_10.restype = None
     lib.dd_measure_popc_peak.argtypes = [vp, C.POINTER(C.c_double)]
+    lib.dd_measure_red_peak.argtypes = [vp, C.POINTER(C.c_double)]
     lib.dd_autotune.argtypes = [vp, C.POINTER(_Tuning)]
     lib.dd_mc_extend.argtypes = [vp, C.POINTER(_Req), C.c_uint64, C.POINTER(C.c_uint64), C.POINTER(_Res)]
     lib.dd_an_candidates.argtypes = [vp, u32, u32, C.POINTER(C.c_uint64), C.c_uint64, C.POINTER(_CandRes)]
@@ -298,6 +299,12 @@ class Context:
     def popc_peak(self) -> float:
         v = C.c_double()
         _check(load().dd_measure_popc_peak(self._h, C.byref(v)))
+        return v.value
+
+    def red_peak(self) -> float:
+        """Shared-memory atomic adds per second (the tcgen05 epilogue's bound)."""
+        v = C.c_double()
+        _check(load().dd_measure_red_peak(self._h, C.byref(v)))
         return v.value
 
     def an_candidates(self, k: int, a_bits: int, capacity: int | None = None) -> tuple[dict, list[int]]:

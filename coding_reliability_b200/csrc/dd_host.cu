@@ -511,8 +511,8 @@ int dd_autotune(dd_context* ctx, dd_tuning* out) {
   q.code = DD_CODE_AN;
   q.mode = DD_MODE_EXHAUSTIVE;
   q.A = 65521;
-  q.n = 17;
-  const uint64_t pairs = (1ull << 17) * ((1ull << 17) - 1) / 2;
+  q.n = 20;  // large enough that every kernel reaches its steady state (0.1 s per run)
+  const uint64_t pairs = (1ull << 20) * ((1ull << 20) - 1) / 2;
   auto best_ms = [&](uint32_t kernel, int mode, double* ms_out) -> int {
     const int saved_mode = ctx->hist_mode, saved_tuned = ctx->tuned;
     ctx->hist_mode = mode;
@@ -661,6 +661,30 @@ int dd_measure_popc_peak(dd_context* ctx, double* popc_per_s) {
   if (e != cudaSuccess) return cuda_fail(e, "popc probe");
   const double popcs = (double)grid * 256.0 * iters * 16.0 * 8.0;
   *popc_per_s = popcs / (best * 1e-3);
+  return DD_OK;
+}
+
+int dd_measure_red_peak(dd_context* ctx, double* adds_per_s) {
+  if (!ctx || !adds_per_s) { set_error("NULL argument"); return DD_ERR_INVALID_ARGUMENT; }
+  DD_CUDA(cudaSetDevice(ctx->device));
+  uint32_t* sink = nullptr;
+  const int grid = ctx->num_sms;
+  DD_CUDA(cudaMalloc(&sink, grid * sizeof(uint32_t)));
+  const uint32_t iters = 20000;
+  cudaError_t e = launch_red_rate(iters / 10, grid, sink, ctx->stream);  // warm-up
+  float best = 1e30f;
+  for (int rep = 0; rep < 3 && e == cudaSuccess; ++rep) {
+    e = cudaEventRecord(ctx->ev0, ctx->stream);
+    if (e == cudaSuccess) e = launch_red_rate(iters, grid, sink, ctx->stream);
+    if (e == cudaSuccess) e = cudaEventRecord(ctx->ev1, ctx->stream);
+    if (e == cudaSuccess) e = cudaEventSynchronize(ctx->ev1);
+    float ms = 0;
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+    if (e == cudaSuccess && ms < best) best = ms;
+  }
+  cudaFree(sink);
+  if (e != cudaSuccess) return cuda_fail(e, "shared-atomic probe");
+  *adds_per_s = (double)red_rate_adds(iters, grid) / (best * 1e-3);
   return DD_OK;
 }
 

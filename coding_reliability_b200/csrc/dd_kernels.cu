@@ -576,6 +576,31 @@ __global__ void __launch_bounds__(256) popc_rate_kernel(uint32_t iters, uint32_t
   if (r == 0x12345678u) sink[blockIdx.x] = r;
 }
 
+// Shared-memory atomic issue rate, as the tcgen05 kernel's epilogue uses it:
+// one CTA of 512 threads per SM, each thread adds 1 to its own column of a
+// 32-row x 512-column table (row stride 2 KB, so a warp's 32 lanes hit 32
+// banks), the row changing with every add.
+constexpr int kRedThreads = 512;
+constexpr int kRedRows = 32;
+
+__global__ void __launch_bounds__(kRedThreads, 1) red_rate_kernel(uint32_t iters, uint32_t* sink) {
+  extern __shared__ uint32_t tab[];  // kRedRows x kRedThreads
+  for (int k = threadIdx.x; k < kRedRows * kRedThreads; k += kRedThreads) tab[k] = 0;
+  __syncthreads();
+  const uint32_t base = (uint32_t)__cvta_generic_to_shared(tab) + threadIdx.x * 4u;
+  for (uint32_t i = 0; i < iters; ++i) {
+#pragma unroll
+    for (int u = 0; u < 32; ++u) {
+      const uint32_t row = (i + (uint32_t)u * 7u) & (kRedRows - 1);
+      asm volatile("red.shared.add.u32 [%0], 1;" ::"r"(base + (row << 11)) : "memory");
+    }
+  }
+  __syncthreads();
+  uint32_t s = 0;
+  for (int r = 0; r < kRedRows; ++r) s += tab[r * kRedThreads + threadIdx.x];
+  if (s != iters * 32u) sink[blockIdx.x] = s;  // never for a correct run; keeps the adds alive
+}
+
 // ---------------------------------------------------------------------------
 // host-callable launchers
 // ---------------------------------------------------------------------------
@@ -607,5 +632,15 @@ cudaError_t launch_popc_rate(uint32_t iters, int grid, uint32_t* sink, cudaStrea
   popc_rate_kernel<<<grid, 256, 0, stream>>>(iters, 0x9e3779b9u, sink);
   return cudaGetLastError();
 }
+
+// One CTA per SM: the table needs 64 KB, the launch asks for more than half an SM.
+cudaError_t launch_red_rate(uint32_t iters, int grid, uint32_t* sink, cudaStream_t stream) {
+  const int smem = 120 * 1024;
+  cudaError_t e = cudaFuncSetAttribute(red_rate_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  if (e != cudaSuccess) return e;
+  red_rate_kernel<<<grid, kRedThreads, smem, stream>>>(iters, sink);
+  return cudaGetLastError();
+}
+uint64_t red_rate_adds(uint32_t iters, int grid) { return (uint64_t)grid * kRedThreads * iters * 32u; }
 
 }  // namespace dd

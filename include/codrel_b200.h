@@ -274,15 +274,20 @@ typedef struct dd_tuning {
   uint64_t probe_pairs;       /* pairs of the probe instance each variant ran */
 } dd_tuning;
 
-/* Times every kernel variant on a probe instance (A = 65521, k = 17: 34-bit
- * codewords, 8.6e9 pairs) on this context's GPU and keeps the fastest for
- * kernel = AUTO.  Runs by itself before the first large AUTO request. */
+/* Times every kernel variant on a probe instance (A = 65521, k = 20: 36-bit
+ * codewords, 5.5e11 pairs, about a second in all) on this context's GPU and
+ * keeps the fastest for kernel = AUTO.  Runs by itself before the first large
+ * AUTO request. */
 int dd_autotune(dd_context* ctx, dd_tuning* out);
 
 /* --- measurement -------------------------------------------------------- */
 /* Measures the device's POPC issue rate (popc/s) with a dependency-free POPC
  * loop on the context's stream. */
 int dd_measure_popc_peak(dd_context* ctx, double* popc_per_s);
+/* Measures the device's shared-memory atomic rate (red.shared.add.u32 per
+ * second, conflict-free, 16 warps per SM): the bound of the tcgen05 path's
+ * histogram epilogue, one atomic per distance. */
+int dd_measure_red_peak(dd_context* ctx, double* adds_per_s);
 
 /* --- super-A candidates --------------------------------------------------- */
 /* Replaces the worker loop of ANcandidates (ANcandidates/ANcandidates.cpp:35-163,

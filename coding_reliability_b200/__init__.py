@@ -170,6 +170,7 @@ def load() -> C.CDLL:
     lib.dd_philox4x32_10.restype = None
     lib.dd_measure_popc_peak.argtypes = [vp, C.POINTER(C.c_double)]
     lib.dd_measure_red_peak.argtypes = [vp, C.POINTER(C.c_double)]
+    lib.dd_set_wait_timeout.argtypes = [vp, C.c_uint64]
     lib.dd_autotune.argtypes = [vp, C.POINTER(_Tuning)]
     lib.dd_mc_extend.argtypes = [vp, C.POINTER(_Req), C.c_uint64, C.POINTER(C.c_uint64), C.POINTER(_Res)]
     lib.dd_an_candidates.argtypes = [vp, u32, u32, C.POINTER(C.c_uint64), C.c_uint64, C.POINTER(_CandRes)]
@@ -300,6 +301,10 @@ class Context:
         v = C.c_double()
         _check(load().dd_measure_popc_peak(self._h, C.byref(v)))
         return v.value
+
+    def set_wait_timeout(self, ns: int) -> None:
+        """Bound of the tcgen05 kernel's device-side waits (0: the 2 s default)."""
+        _check(load().dd_set_wait_timeout(self._h, ns))
 
     def red_peak(self) -> float:
         """Shared-memory atomic adds per second (the tcgen05 epilogue's bound)."""

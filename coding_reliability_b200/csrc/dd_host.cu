@@ -664,6 +664,12 @@ int dd_measure_popc_peak(dd_context* ctx, double* popc_per_s) {
   return DD_OK;
 }
 
+int dd_set_wait_timeout(dd_context* ctx, uint64_t ns) {
+  if (!ctx) { set_error("NULL argument"); return DD_ERR_INVALID_ARGUMENT; }
+  ctx->mma_timeout_ns = ns ? ns : 2000000000ull;
+  return DD_OK;
+}
+
 int dd_measure_red_peak(dd_context* ctx, double* adds_per_s) {
   if (!ctx || !adds_per_s) { set_error("NULL argument"); return DD_ERR_INVALID_ARGUMENT; }
   DD_CUDA(cudaSetDevice(ctx->device));

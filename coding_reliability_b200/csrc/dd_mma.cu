@@ -55,6 +55,9 @@ constexpr int kBTileBytes = kN * kK;    // 8 KB
 constexpr int kBBytes = kTilesPerStrip * kBTileBytes;  // 64 KB
 constexpr uint32_t kTmemCols = 512;
 constexpr uint32_t kMinSmem = 120 * 1024;  // more than half an SM: one CTA (and one TMEM owner) per SM
+// Bound of the wait for in-flight MMAs before an aborted CTA releases its TMEM;
+// fixed, independent of MmaArgs::timeout_ns (which a caller may set very short).
+constexpr unsigned long long kDrainTimeoutNs = 2000000000ull;
 constexpr int kBufs = kTmemCols / kN;   // 4 accumulator buffers
 constexpr int kColsPerWarp = kN / (kEpiWarps / 4);  // 32: each epilogue warp reads one 32-column load per tile
 static_assert(kEpiWarps % 4 == 0 && kColsPerWarp == 32, "one 32-column TMEM load per warp and tile");
@@ -450,7 +453,7 @@ __global__ void __launch_bounds__(kThreads, 1) mma_hist_kernel(MmaArgs args) {
         *abort = 1u;
         atomicOr(args.status, KSTATUS_TIMEOUT);
         // let the last MMA drain (bounded, in-order completion) before TMEM is released
-        if (g > 0) mbar_wait_bounded(smem_u32(&sh->full[(g - 1) & 3]), (uint32_t)((g - 1) >> 2) & 1u, args.timeout_ns);
+        if (g > 0) mbar_wait_bounded(smem_u32(&sh->full[(g - 1) & 3]), (uint32_t)((g - 1) >> 2) & 1u, kDrainTimeoutNs);
       }
     }
     __syncwarp();

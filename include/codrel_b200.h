@@ -289,6 +289,14 @@ int dd_measure_popc_peak(dd_context* ctx, double* popc_per_s);
  * histogram epilogue, one atomic per distance. */
 int dd_measure_red_peak(dd_context* ctx, double* adds_per_s);
 
+/* --- failure detection -------------------------------------------------- */
+/* Bound (ns) of every device-side wait of this context's tcgen05 launches;
+ * 0 restores the default of 2 s.  A wait that runs out makes the kernel stop,
+ * release its tensor memory and report DD_ERR_TIMEOUT; the context stays
+ * usable.  A very short bound makes the first wait run out, which is how the
+ * timeout path is tested without a fault or a hang. */
+int dd_set_wait_timeout(dd_context* ctx, uint64_t ns);
+
 /* --- super-A candidates --------------------------------------------------- */
 /* Replaces the worker loop of ANcandidates (ANcandidates/ANcandidates.cpp:35-163,
  * main :236-301): for every odd A with exactly a_bits bits the smallest

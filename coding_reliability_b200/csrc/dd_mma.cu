@@ -212,14 +212,6 @@ __device__ __forceinline__ uint32_t find_job(const Job* jobs, uint32_t njobs, ui
   return lo;
 }
 
-// One TMEM buffer's tile, published by the issuer with its MMA.
-struct TileInfo {
-  unsigned long long r0;  // first row (codeword index) of the strip
-  unsigned long long c0;  // first column of this N = 128 tile
-  unsigned long long n;   // codewords of the job
-  uint32_t job;           // job index
-  uint32_t flags;         // kInfoDone | kInfoFull
-};
 constexpr uint32_t kInfoDone = 1u, kInfoFull = 2u;
 
 // One strip (128 rows x one super tile of columns) as the generators publish it.
@@ -231,7 +223,10 @@ struct StripInfo {
 struct Shared {
   uint64_t full[kBufs];   // tile in TMEM buffer b ready: tcgen05.commit + the issuer's arrive (count 2)
   uint64_t empty[kBufs];  // TMEM buffer b read: one arrive per epilogue warp (count kEpiWarps)
-  TileInfo info[kBufs];
+  // strip info for the epilogue, by issued strip (tile g belongs to strip g / kTilesPerStrip):
+  // read once per strip, so the epilogue's per-tile shared-memory traffic is the
+  // barrier poll and arrive only (its loads would queue behind the atomics)
+  StripInfo estrip[2];
   // strip queue, generators -> issuer (slot = strip & 1, with that slot's row operand)
   StripInfo strip[2];
   uint64_t slot_full[2];  // strip ready: the generators' thread 0 arrives (count 1)
@@ -272,7 +267,8 @@ __device__ __forceinline__ bool wait_or_abort(uint32_t addr, uint32_t parity, un
 // Warp roles: warps 0..15 bin (epilogue), warp 16 issues the MMAs (lane 0),
 // warps 17..19 claim strips and write their operands.  Hand-offs go through
 // mbarriers only: slot_full/slot_free (a strip's operands written / its MMAs
-// done), full[b] (the MMA result in TMEM buffer b and its TileInfo are ready),
+// done), full[b] (the MMA result in TMEM buffer b is ready, and for a strip's
+// first tile the strip's StripInfo),
 // empty[b] (all 16 epilogue warps have read buffer b).  No CTA-wide barrier
 // runs between set-up and exit.
 //
@@ -426,12 +422,12 @@ __global__ void __launch_bounds__(kThreads, 1) mma_hist_kernel(MmaArgs args) {
         for (int tile = 0; tile < kTilesPerStrip; ++tile, ++g) {
           if (!wait_empty(g)) { ok = false; break; }
           const uint32_t b = (uint32_t)(g & 3);
-          TileInfo& ti = sh->info[b];
-          ti.r0 = si.r0;
-          ti.c0 = si.c0 + (uint64_t)tile * kN;
-          ti.n = si.n;
-          ti.job = si.job;
-          ti.flags = si.flags & kInfoFull;
+          if (tile == 0) {
+            // the entry of strip s-2: every warp read it at tile g-16 < g-4
+            StripInfo& es = sh->estrip[(g / kTilesPerStrip) & 1];
+            es = si;
+            es.flags = si.flags & kInfoFull;
+          }
           tc_fence_after();
           const uint32_t d = tmem + b * (uint32_t)kN;
           const uint32_t b0 = smem_u32(sB + tile * kBTileBytes);
@@ -445,8 +441,8 @@ __global__ void __launch_bounds__(kThreads, 1) mma_hist_kernel(MmaArgs args) {
         mma_commit(smem_u32(&sh->slot_free[slot]));  // the strip's operands are free once its MMAs are done
       }
       if (normal && wait_empty(g)) {
-        // end of work: a tile marked done wakes the epilogue warps
-        sh->info[g & 3].flags = kInfoDone;
+        // end of work: a strip marked done wakes the epilogue warps (g is a strip's first tile)
+        sh->estrip[(g / kTilesPerStrip) & 1].flags = kInfoDone;
         mbar_arrive(smem_u32(&sh->full[g & 3]));
         mbar_arrive(smem_u32(&sh->full[g & 3]));
       } else {
@@ -476,20 +472,28 @@ __global__ void __launch_bounds__(kThreads, 1) mma_hist_kernel(MmaArgs args) {
         }
       }
     };
+    unsigned long long r0 = 0, cs = 0, n = 0;  // the current strip: first row, first column, codewords
+    uint32_t flags = 0, job = 0;
     for (uint64_t g = 0;; ++g) {
       const uint32_t b = (uint32_t)(g & 3);
       bool r = true;
       if (lane == 0) r = wait_or_abort(smem_u32(&sh->full[b]), (uint32_t)(g >> 2) & 1u, args.timeout_ns, abort);
       if (!__shfl_sync(0xffffffffu, r ? 1 : 0, 0)) { ok = false; break; }
-      __syncwarp();  // lane 0's wait acquired the issuer's TileInfo; this orders it for the warp
-      const TileInfo& ti = sh->info[b];
-      const uint32_t flags = ti.flags;
-      if (flags & kInfoDone) break;
-      const uint32_t job = ti.job;
+      __syncwarp();  // lane 0's wait acquired the MMA result (and StripInfo); this orders it for the warp
+      const uint32_t tile = (uint32_t)(g % kTilesPerStrip);
+      if (tile == 0) {
+        const StripInfo& es = sh->estrip[(g / kTilesPerStrip) & 1];
+        flags = es.flags;
+        if (flags & kInfoDone) break;
+        job = es.job;
+        r0 = es.r0;
+        cs = es.c0;
+        n = es.n;
+      }
       tc_fence_after();
       uint32_t v[32];
       tmem_ld32_nowait(tmem + ((uint32_t)(q * 32) << 16) + b * (uint32_t)kN + (uint32_t)(sub * kColsPerWarp), v);
-      const unsigned long long r0 = ti.r0, c0 = ti.c0, n = ti.n;
+      const unsigned long long c0 = cs + (unsigned long long)tile * kN;
       tmem_wait_ld();
       // the buffer may be refilled as soon as every warp has its values in registers
       tc_fence_before();

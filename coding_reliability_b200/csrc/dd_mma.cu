@@ -11,9 +11,11 @@
 //
 // Work unit: the popc kernel's tile space (1024x1024 super tiles of the i<j
 // triangle, split into 8 strips of 128 rows).  A strip is 128 rows (UMMA M) x
-// 1024 columns = 8 MMA tiles of N = 128, accumulated in four TMEM buffers of 128
-// columns, so the epilogue may trail the MMAs by three tiles before the issuer
-// has to wait for it.  Generator warps claim 8 strips at a time (one super tile
+// 1024 columns = 4 MMA tiles of N = 256, accumulated in two TMEM buffers of 256
+// columns: the MMA of tile t+1 runs while the epilogue bins tile t.  (Four
+// buffers of N = 128 measured 17 % slower: every tile costs each epilogue warp
+// a barrier poll and an arrive through the shared-memory pipe that its atomics
+// saturate, so fewer, wider tiles win over deeper buffering.)  Generator warps claim 8 strips at a time (one super tile
 // when the job's tile range is aligned), so the column operand of a super tile
 // is written once for its 8 strips; the row operand is double-buffered by strip
 // and written while the previous strip's MMAs run.
@@ -45,23 +47,25 @@ constexpr int kGenWarps = 3;                           // warps 17..19: claim, d
 constexpr int kGenThreads = kGenWarps * 32;
 constexpr int kThreads = kEpiThreads + 32 + kGenThreads;
 constexpr int kM = 128;                 // rows per strip (UMMA M)
-constexpr int kN = 128;                 // columns per MMA tile (UMMA N)
-constexpr int kTilesPerStrip = kSuper / kN;  // 8
+constexpr int kN = 256;                 // columns per MMA tile (UMMA N)
+constexpr int kTilesPerStrip = kSuper / kN;  // 4
 constexpr int kK = 64;                  // bytes of K per row/column
 constexpr int kLBO = 128;               // bytes between K-adjacent 8x16B core matrices
 constexpr int kSBO = 512;               // bytes between M/N-adjacent 8-row groups (4 core matrices)
 constexpr int kABytes = kM * kK;        // 8 KB
-constexpr int kBTileBytes = kN * kK;    // 8 KB
+constexpr int kBTileBytes = kN * kK;    // 16 KB
 constexpr int kBBytes = kTilesPerStrip * kBTileBytes;  // 64 KB
 constexpr uint32_t kTmemCols = 512;
 constexpr uint32_t kMinSmem = 120 * 1024;  // more than half an SM: one CTA (and one TMEM owner) per SM
 // Bound of the wait for in-flight MMAs before an aborted CTA releases its TMEM;
 // fixed, independent of MmaArgs::timeout_ns (which a caller may set very short).
 constexpr unsigned long long kDrainTimeoutNs = 2000000000ull;
-constexpr int kBufs = kTmemCols / kN;   // 4 accumulator buffers
-constexpr int kColsPerWarp = kN / (kEpiWarps / 4);  // 32: each epilogue warp reads one 32-column load per tile
-static_assert(kEpiWarps % 4 == 0 && kColsPerWarp == 32, "one 32-column TMEM load per warp and tile");
-static_assert(kBufs == 4, "buffer index and phase arithmetic below assume 4 buffers");
+constexpr int kBufs = kTmemCols / kN;   // accumulator buffers
+constexpr int kColsPerWarp = kN / (kEpiWarps / 4);  // columns of a tile each epilogue warp reads
+constexpr int kLoads = kColsPerWarp / 32;           // 32-column TMEM loads per warp and tile
+static_assert(kEpiWarps % 4 == 0 && kColsPerWarp % 32 == 0, "whole 32-column TMEM loads per warp and tile");
+__host__ __device__ constexpr uint32_t buf_of(uint64_t g) { return (uint32_t)(g % kBufs); }
+__host__ __device__ constexpr uint32_t parity_of(uint64_t g) { return (uint32_t)(g / kBufs) & 1u; }
 
 // ---------------------------------------------------------------- PTX wrappers
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -123,7 +127,7 @@ __device__ __forceinline__ uint64_t smem_desc(uint32_t addr) {
   return d;  // base offset 0, absolute-LBO mode off, layout type 0 (SWIZZLE_NONE)
 }
 
-// Instruction descriptor: D = S32, A = B = signed 8-bit, both K-major, M=128, N=128.
+// Instruction descriptor: D = S32, A = B = signed 8-bit, both K-major, M=128, N=kN.
 constexpr uint32_t kIdesc = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(kN >> 3) << 17) |
                             ((uint32_t)(kM >> 4) << 24);
 
@@ -272,8 +276,8 @@ __device__ __forceinline__ bool wait_or_abort(uint32_t addr, uint32_t parity, un
 // empty[b] (all 16 epilogue warps have read buffer b).  No CTA-wide barrier
 // runs between set-up and exit.
 //
-// Epilogue warp w reads TMEM lanes 32*(w%4).. (its rows) and 32 columns
-// 32*(w/4).. of each 128-column tile, and bumps one shared-memory counter per
+// Epilogue warp w reads TMEM lanes 32*(w%4).. (its rows) and 64 columns
+// 64*(w/4).. of each 256-column tile, and bumps one shared-memory counter per
 // pair in its own bin columns (row stride kEpiThreads words), so warps never
 // share a counter and each warp flushes its own columns.  A distance is at
 // most L (both operands have L bit planes, popc(x) <= L), and there are at
@@ -410,7 +414,7 @@ __global__ void __launch_bounds__(kThreads, 1) mma_hist_kernel(MmaArgs args) {
       // until the epilogue has read tile gg-4, the previous tile of gg's buffer
       auto wait_empty = [&](uint64_t gg) -> bool {
         return gg < kBufs ||
-               wait_or_abort(smem_u32(&sh->empty[gg & 3]), (uint32_t)((gg - kBufs) >> 2) & 1u, args.timeout_ns, abort);
+               wait_or_abort(smem_u32(&sh->empty[buf_of(gg)]), parity_of(gg - kBufs), args.timeout_ns, abort);
       };
       for (uint64_t s = 0;; ++s) {
         const uint32_t slot = (uint32_t)(s & 1);
@@ -421,7 +425,7 @@ __global__ void __launch_bounds__(kThreads, 1) mma_hist_kernel(MmaArgs args) {
         bool ok = true;
         for (int tile = 0; tile < kTilesPerStrip; ++tile, ++g) {
           if (!wait_empty(g)) { ok = false; break; }
-          const uint32_t b = (uint32_t)(g & 3);
+          const uint32_t b = buf_of(g);
           if (tile == 0) {
             // the entry of strip s-2: every warp read it at tile g-16 < g-4
             StripInfo& es = sh->estrip[(g / kTilesPerStrip) & 1];
@@ -443,13 +447,13 @@ __global__ void __launch_bounds__(kThreads, 1) mma_hist_kernel(MmaArgs args) {
       if (normal && wait_empty(g)) {
         // end of work: a strip marked done wakes the epilogue warps (g is a strip's first tile)
         sh->estrip[(g / kTilesPerStrip) & 1].flags = kInfoDone;
-        mbar_arrive(smem_u32(&sh->full[g & 3]));
-        mbar_arrive(smem_u32(&sh->full[g & 3]));
+        mbar_arrive(smem_u32(&sh->full[buf_of(g)]));
+        mbar_arrive(smem_u32(&sh->full[buf_of(g)]));
       } else {
         *abort = 1u;
         atomicOr(args.status, KSTATUS_TIMEOUT);
         // let the last MMA drain (bounded, in-order completion) before TMEM is released
-        if (g > 0) mbar_wait_bounded(smem_u32(&sh->full[(g - 1) & 3]), (uint32_t)((g - 1) >> 2) & 1u, kDrainTimeoutNs);
+        if (g > 0) mbar_wait_bounded(smem_u32(&sh->full[buf_of(g - 1)]), parity_of(g - 1), kDrainTimeoutNs);
       }
     }
     __syncwarp();
@@ -475,9 +479,9 @@ __global__ void __launch_bounds__(kThreads, 1) mma_hist_kernel(MmaArgs args) {
     unsigned long long r0 = 0, cs = 0, n = 0;  // the current strip: first row, first column, codewords
     uint32_t flags = 0, job = 0;
     for (uint64_t g = 0;; ++g) {
-      const uint32_t b = (uint32_t)(g & 3);
+      const uint32_t b = buf_of(g);
       bool r = true;
-      if (lane == 0) r = wait_or_abort(smem_u32(&sh->full[b]), (uint32_t)(g >> 2) & 1u, args.timeout_ns, abort);
+      if (lane == 0) r = wait_or_abort(smem_u32(&sh->full[b]), parity_of(g), args.timeout_ns, abort);
       if (!__shfl_sync(0xffffffffu, r ? 1 : 0, 0)) { ok = false; break; }
       __syncwarp();  // lane 0's wait acquired the MMA result (and StripInfo); this orders it for the warp
       const uint32_t tile = (uint32_t)(g % kTilesPerStrip);
@@ -491,8 +495,11 @@ __global__ void __launch_bounds__(kThreads, 1) mma_hist_kernel(MmaArgs args) {
         n = es.n;
       }
       tc_fence_after();
-      uint32_t v[32];
-      tmem_ld32_nowait(tmem + ((uint32_t)(q * 32) << 16) + b * (uint32_t)kN + (uint32_t)(sub * kColsPerWarp), v);
+      uint32_t v[kLoads][32];
+#pragma unroll
+      for (int h = 0; h < kLoads; ++h)
+        tmem_ld32_nowait(tmem + ((uint32_t)(q * 32) << 16) + b * (uint32_t)kN + (uint32_t)(sub * kColsPerWarp + 32 * h),
+                         v[h]);
       const unsigned long long c0 = cs + (unsigned long long)tile * kN;
       tmem_wait_ld();
       // the buffer may be refilled as soon as every warp has its values in registers
@@ -508,15 +515,19 @@ __global__ void __launch_bounds__(kThreads, 1) mma_hist_kernel(MmaArgs args) {
       }
       if (flags & kInfoFull) {
 #pragma unroll
-        for (int u = 0; u < 32; ++u) red_shared(hist_lane + (v[u] << 11));
+        for (int h = 0; h < kLoads; ++h)
+#pragma unroll
+          for (int u = 0; u < 32; ++u) red_shared(hist_lane + (v[h][u] << 11));
       } else {
         const uint64_t i = r0 + (uint64_t)(q * 32 + lane);
         const uint64_t j0 = c0 + (uint64_t)(sub * kColsPerWarp);
 #pragma unroll
-        for (int u = 0; u < 32; ++u) {
-          const uint64_t j = j0 + u;
-          if (i < n && j < n && j > i) red_shared(hist_lane + (v[u] << 11));
-        }
+        for (int h = 0; h < kLoads; ++h)
+#pragma unroll
+          for (int u = 0; u < 32; ++u) {
+            const uint64_t j = j0 + 32 * h + u;
+            if (i < n && j < n && j > i) red_shared(hist_lane + (v[h][u] << 11));
+          }
       }
       if (++since_flush >= kFlushEvery) { flush(); since_flush = 0; }
     }

@@ -251,16 +251,20 @@ __device__ __forceinline__ void mbar_arrive(uint32_t addr) {
 
 // Bounded wait (single thread): true when the phase completed; false after
 // timeout_ns or once another thread has aborted (then this one aborts too).
+// The abort flag (shared memory) and the timer are checked every 32 polls: the
+// polls themselves go through the shared-memory pipe the epilogue's atomics load.
 __device__ __forceinline__ bool wait_or_abort(uint32_t addr, uint32_t parity, unsigned long long timeout_ns,
                                               volatile uint32_t* abort) {
   if (mbar_try_wait(addr, parity)) return true;
   const uint64_t t0 = globaltimer();
-  while (true) {
+  for (uint32_t spin = 1;; ++spin) {
     if (mbar_try_wait(addr, parity)) return true;
-    if (*abort) return false;
-    if (globaltimer() - t0 > timeout_ns) {
-      *abort = 1u;
-      return false;
+    if ((spin & 31) == 0) {
+      if (*abort) return false;
+      if (globaltimer() - t0 > timeout_ns) {
+        *abort = 1u;
+        return false;
+      }
     }
   }
 }

@@ -124,4 +124,11 @@ __host__ __device__ __forceinline__ uint64_t mc_index(uint64_t seed, uint64_t id
   return n == 64 ? r : (r >> (64 - n));
 }
 
+// Grid lattice codeword: v = A * (T)(k * stepsize), T = uint32 or uint64 as the
+// reference's Caller picks it (src/an_coding_grid.cu:83-106).
+__host__ __device__ __forceinline__ uint64_t lattice_value(uint64_t A, uint64_t k, double step, uint32_t t32) {
+  if (t32) return (uint64_t)(uint32_t)(A * (uint64_t)(uint32_t)((double)k * step));
+  return A * (uint64_t)((double)k * step);
+}
+
 }  // namespace dd

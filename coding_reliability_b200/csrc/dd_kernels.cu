@@ -96,12 +96,6 @@ __device__ __forceinline__ void flush_bins(uint32_t* wbins, unsigned long long* 
 // ---------------------------------------------------------------------------
 // generators
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ uint64_t lattice_value(uint64_t A, uint64_t k, double step, uint32_t t32) {
-  // v = A * (T)(k * stepsize), T = uint32 or uint64 as the reference's Caller picks it.
-  if (t32) return (uint64_t)(uint32_t)(A * (uint64_t)(uint32_t)((double)k * step));
-  return A * (uint64_t)((double)k * step);
-}
-
 __device__ __forceinline__ uint64_t row_value(const Job& J, uint64_t i) {
   switch (J.row_kind) {
     case ROW_LATTICE: return lattice_value(J.A, i, J.row_step, J.t32);

@@ -10,7 +10,8 @@
 // per pair; no other per-pair arithmetic is left.
 //
 // Work unit: the popc kernel's tile space (1024x1024 super tiles of the i<j
-// triangle, split into 8 strips of 128 rows).  A strip is 128 rows (UMMA M) x
+// triangle, split into 8 strips of 128 rows; for grid jobs, 128 lattice rows x
+// 1024 columns, taken column-major).  A strip is 128 rows (UMMA M) x
 // 1024 columns = 4 MMA tiles of N = 256, accumulated in two TMEM buffers of 256
 // columns: the MMA of tile t+1 runs while the epilogue bins tile t.  (Four
 // buffers of N = 128 measured 17 % slower: every tile costs each epilogue warp
@@ -216,13 +217,26 @@ __device__ __forceinline__ uint32_t find_job(const Job* jobs, uint32_t njobs, ui
   return lo;
 }
 
-constexpr uint32_t kInfoDone = 1u, kInfoFull = 2u;
+constexpr uint32_t kInfoDone = 1u, kInfoFull = 2u, kInfoRect = 4u;
 
 // One strip (128 rows x one super tile of columns) as the generators publish it.
 struct StripInfo {
-  unsigned long long r0, c0, n;
-  uint32_t job, flags;  // kInfoDone | kInfoFull
+  unsigned long long r0, c0;
+  unsigned long long n;     // rows (codewords of a triangle job, lattice points of a grid job)
+  unsigned long long cols;  // columns
+  uint32_t job, flags;      // kInfoDone | kInfoFull | kInfoRect
 };
+
+// Codeword of row i / column j of job J: A*i for the codeword progression, the
+// lattice codeword for grid rows and (2-D) columns.
+__device__ __forceinline__ uint64_t mma_row_value(const Job* J, uint64_t i) {
+  return __ldg(&J->row_kind) == ROW_LATTICE ? lattice_value(__ldg(&J->A), i, __ldg(&J->row_step), __ldg(&J->t32))
+                                            : __ldg(&J->A) * i;
+}
+__device__ __forceinline__ uint64_t mma_col_value(const Job* J, uint64_t j) {
+  return __ldg(&J->col_kind) == COL_LATTICE ? lattice_value(__ldg(&J->A), j, __ldg(&J->col_step), __ldg(&J->t32))
+                                            : __ldg(&J->A) * j;
+}
 
 struct Shared {
   uint64_t full[kBufs];   // tile in TMEM buffer b ready: tcgen05.commit + the issuer's arrive (count 2)
@@ -348,15 +362,29 @@ __global__ void __launch_bounds__(kThreads, 1) mma_hist_kernel(MmaArgs args) {
         if (gtid == 0) atomicOr(args.status, KSTATUS_BAD_JOB);
         continue;
       }
-      const uint64_t A = __ldg(&jp->A), N = __ldg(&jp->rows);
+      const uint64_t A = __ldg(&jp->A), N = __ldg(&jp->rows), NC = __ldg(&jp->cols);
       const uint64_t lt = tt - tb + __ldg(&jp->tile_offset);
-      uint64_t sr, sc;
-      tri_decode(lt / kStrips, __ldg(&jp->col_tiles), sr, sc);
-      const uint64_t r0 = sr * kSuper + (lt % kStrips) * kM;
-      const uint64_t c0 = sc * kSuper;
+      const bool rect = __ldg(&jp->shape) == SHAPE_RECT;
+      uint64_t r0, c0, sc;
+      bool full;
+      if (rect) {
+        // grid job: 128 rows x 1024 columns per tile, column-major here so that
+        // consecutive tiles share the column operand
+        const uint64_t row_tiles = (N + kM - 1) / kM;
+        sc = lt / row_tiles;
+        r0 = (lt % row_tiles) * kM;
+        c0 = sc * kSuper;
+        full = (r0 + kM <= N) && (c0 + kSuper <= NC);
+      } else {
+        uint64_t sr;
+        tri_decode(lt / kStrips, __ldg(&jp->col_tiles), sr, sc);
+        r0 = sr * kSuper + (lt % kStrips) * kM;
+        c0 = sc * kSuper;
+        full = (r0 + kM <= N) && (c0 + kSuper <= N) && sr != sc;
+      }
       if (r0 >= N) continue;  // uniform over the group
-      const bool full = (r0 + kM <= N) && (c0 + kSuper <= N) && sr != sc;
-      const uint64_t maxcw = A * (N - 1);
+      // every codeword of the job lies below A * 2^n (lattice points are indices < 2^n)
+      const uint64_t maxcw = A * ((1ull << __ldg(&jp->n)) - 1ull);
       int L = 64 - __clzll((long long)(maxcw | 1));
       L = (L + 3) & ~3;
       const uint32_t slot = (uint32_t)(s & 1);
@@ -378,7 +406,8 @@ __global__ void __launch_bounds__(kThreads, 1) mma_hist_kernel(MmaArgs args) {
 #pragma unroll 1
         for (int cc = gtid; cc < kSuper; cc += kGenThreads) {
           const uint64_t j = c0 + cc;
-          write_operand(sB + (cc / kN) * kBTileBytes, cc % kN, j < N ? A * j : 0, L, false);
+          write_operand(sB + (cc / kN) * kBTileBytes, cc % kN, j < (rect ? NC : N) ? mma_col_value(jp, j) : 0, L,
+                        false);
         }
         bjob = jn;
         bsc = sc;
@@ -387,7 +416,7 @@ __global__ void __launch_bounds__(kThreads, 1) mma_hist_kernel(MmaArgs args) {
 #pragma unroll 1
       for (int rr = gtid; rr < kM; rr += kGenThreads) {
         const uint64_t i = r0 + rr;
-        write_operand(a, rr, i < N ? A * i : 0, L, true);
+        write_operand(a, rr, i < N ? mma_row_value(jp, i) : 0, L, true);
       }
       fence_proxy_async();
       gen_bar();  // both operands complete
@@ -396,8 +425,9 @@ __global__ void __launch_bounds__(kThreads, 1) mma_hist_kernel(MmaArgs args) {
         si.r0 = r0;
         si.c0 = c0;
         si.n = N;
+        si.cols = rect ? NC : N;
         si.job = jn;
-        si.flags = full ? kInfoFull : 0u;
+        si.flags = (full ? kInfoFull : 0u) | (rect ? kInfoRect : 0u);
         mbar_arrive(smem_u32(&sh->slot_full[slot]));
       }
       ++s;
@@ -434,7 +464,7 @@ __global__ void __launch_bounds__(kThreads, 1) mma_hist_kernel(MmaArgs args) {
             // the entry of strip s-2: every warp read it at tile g-16 < g-4
             StripInfo& es = sh->estrip[(g / kTilesPerStrip) & 1];
             es = si;
-            es.flags = si.flags & kInfoFull;
+            es.flags = si.flags & (kInfoFull | kInfoRect);
           }
           tc_fence_after();
           const uint32_t d = tmem + b * (uint32_t)kN;
@@ -480,7 +510,7 @@ __global__ void __launch_bounds__(kThreads, 1) mma_hist_kernel(MmaArgs args) {
         }
       }
     };
-    unsigned long long r0 = 0, cs = 0, n = 0;  // the current strip: first row, first column, codewords
+    unsigned long long r0 = 0, cs = 0, n = 0, nc = 0;  // the current strip: first row and column, rows, columns
     uint32_t flags = 0, job = 0;
     for (uint64_t g = 0;; ++g) {
       const uint32_t b = buf_of(g);
@@ -497,6 +527,7 @@ __global__ void __launch_bounds__(kThreads, 1) mma_hist_kernel(MmaArgs args) {
         r0 = es.r0;
         cs = es.c0;
         n = es.n;
+        nc = es.cols;
       }
       tc_fence_after();
       uint32_t v[kLoads][32];
@@ -530,7 +561,8 @@ __global__ void __launch_bounds__(kThreads, 1) mma_hist_kernel(MmaArgs args) {
 #pragma unroll
           for (int u = 0; u < 32; ++u) {
             const uint64_t j = j0 + 32 * h + u;
-            if (i < n && j < n && j > i) red_shared(hist_lane + (v[h][u] << 11));
+            const bool in = (flags & kInfoRect) ? (i < n && j < nc) : (i < n && j < n && j > i);
+            if (in) red_shared(hist_lane + (v[h][u] << 11));
           }
       }
       if (++since_flush >= kFlushEvery) { flush(); since_flush = 0; }
@@ -546,10 +578,10 @@ __global__ void __launch_bounds__(kThreads, 1) mma_hist_kernel(MmaArgs args) {
 }
 
 // ---------------------------------------------------------------- host side
-// Bit planes of the operands of job j: the bits of its largest codeword, rounded
-// up to 4 (the kernel computes the same from the job).
+// Bit planes of the operands of job j: the bits of A * (2^n - 1), which bounds
+// every codeword of the job, rounded up to 4 (the kernel computes the same).
 int mma_operand_bits(const Job& j) {
-  const unsigned __int128 maxcw = (unsigned __int128)j.A * (j.rows - 1);
+  const unsigned __int128 maxcw = (unsigned __int128)j.A * ((1ull << j.n) - 1ull);
   int bits = 0;
   for (unsigned __int128 v = maxcw; v; v >>= 1) ++bits;
   if (bits == 0) bits = 1;
@@ -557,13 +589,11 @@ int mma_operand_bits(const Job& j) {
 }
 
 bool mma_eligible(const Job& j) {
-  if (j.kind != JOB_PAIRS || j.shape != SHAPE_TRIANGLE || j.row_kind != ROW_PROGRESSION ||
-      j.col_kind != COL_PROGRESSION)
-    return false;
-  const unsigned __int128 maxcw = (unsigned __int128)j.A * (j.rows - 1);
-  int bits = 0;
-  for (unsigned __int128 v = maxcw; v; v >>= 1) ++bits;
-  return ((bits + 3) & ~3) <= 60;
+  if (j.kind != JOB_PAIRS || j.n > 48) return false;
+  const bool tri = j.shape == SHAPE_TRIANGLE && j.row_kind == ROW_PROGRESSION && j.col_kind == COL_PROGRESSION;
+  const bool rect = j.shape == SHAPE_RECT && (j.row_kind == ROW_PROGRESSION || j.row_kind == ROW_LATTICE) &&
+                    (j.col_kind == COL_PROGRESSION || j.col_kind == COL_LATTICE) && j.col_tiles * kSuper >= j.cols;
+  return (tri || rect) && mma_operand_bits(j) <= 60;
 }
 
 size_t mma_smem_bytes(uint32_t hist_rows) {

@@ -57,3 +57,42 @@ def test_mma_k24_archive_A63877(ctx):
     case = next(c for c in golden("an_exhaustive.json") if c["A"] == 63877 and c["n"] == 24)
     res = ctx.histogram(mma_req(63877, 24))
     assert res.counts == case["counts"]
+
+
+# -- grid jobs on the tcgen05 path (lattice rows x codeword / lattice columns) -----
+@pytest.mark.parametrize("A,n,m", [(61, 12, 3), (61, 12, 17), (641, 14, 1000), (58659, 16, 4096), (58659, 18, 77),
+                                   (3, 10, 1024), (65521, 17, 333), (58659, 20, 1 << 12)])
+def test_mma_grid1d_vs_oracle_and_popc(ctx, A, n, m):
+    req = dd.Request(dd.CODE_AN, dd.MODE_GRID_1D, A, n, m=m, kernel=dd.KERNEL_MMA)
+    nb, h, Aeff = dd.request_shape(req)
+    res = ctx.histogram(req)
+    assert res.kernel_used == dd.KERNEL_MMA
+    popc = ctx.histogram(dd.Request(dd.CODE_AN, dd.MODE_GRID_1D, A, n, m=m, kernel=dd.KERNEL_POPC))
+    assert res.raw == popc.raw and res.counts == popc.counts
+    if n <= 18:
+        raw, _ = oracle.an_grid1d_raw(Aeff, n, h, m, nb)
+        assert res.raw == raw
+
+
+@pytest.mark.parametrize("A,n,m,m2", [(61, 12, 100, 37), (641, 14, 64, 64), (58659, 18, 50, 300), (3, 8, 256, 1),
+                                      (61, 40, 1000, 1000), (58659, 40, 4096, 512), (641, 36, 999, 1001)])
+def test_mma_grid2d_vs_oracle(ctx, A, n, m, m2):
+    req = dd.Request(dd.CODE_AN, dd.MODE_GRID_2D, A, n, m=m, m2=m2, kernel=dd.KERNEL_MMA)
+    nb, h, Aeff = dd.request_shape(req)
+    res = ctx.histogram(req)
+    assert res.kernel_used == dd.KERNEL_MMA
+    raw = oracle.an_grid2d_raw(Aeff, n, m, m2, nb)
+    assert res.raw[1:] == raw[1:] and res.raw[0] == 0
+    assert res.counts == oracle.an_grid_counts(2, n, min(m, 1 << n), min(m2, 1 << n), raw)
+
+
+def test_mma_grid_archive(ctx):
+    """Archived 1-D grid histograms of the reference (results/GridMs, converge/geom)."""
+    checked = 0
+    for x in golden("an_grid1d.json"):
+        if x["n"] > 24 or any(isinstance(c, str) for c in x["counts"]):
+            continue
+        res = ctx.histogram(dd.Request(dd.CODE_AN, dd.MODE_GRID_1D, x["A"], x["n"], m=x["m"], kernel=dd.KERNEL_MMA))
+        assert res.counts == x["counts"], x["file"]
+        checked += 1
+    assert checked >= 90

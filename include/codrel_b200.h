@@ -64,7 +64,8 @@ typedef enum dd_mode {
   DD_MODE_MONTE_CARLO = 3  /* Philox4x32-10 sampled pairs (replaces cuRAND Sobol32) */
 } dd_mode;
 
-/* Which kernel family computes an AN exhaustive histogram. */
+/* Which kernel family computes an AN exhaustive or grid histogram (Monte Carlo,
+ * Ext-Hamming and anything wider than 60-bit operands use the popc kernel). */
 typedef enum dd_kernel {
   DD_KERNEL_AUTO = 0,  /* autotuner's choice for the shape */
   DD_KERNEL_POPC = 1,  /* XOR + POPC, warp-private shared-memory bins */
@@ -188,7 +189,7 @@ int dd_mc_extend(dd_context* ctx, const dd_request* req, uint64_t it_done, const
 /* --- batch -------------------------------------------------------------- */
 typedef struct dd_batch_options {
   uint32_t use_graph;       /* capture the launch in a CUDA graph and replay it */
-  uint32_t kernel;          /* dd_kernel for every AN exhaustive instance (AUTO: autotuner) */
+  uint32_t kernel;          /* dd_kernel for every AN exhaustive / grid instance (AUTO: autotuner) */
   uint32_t ctas_per_sm;     /* 0: autotuner */
   uint32_t reserved;
 } dd_batch_options;

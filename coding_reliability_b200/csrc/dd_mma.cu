@@ -228,14 +228,21 @@ struct StripInfo {
 };
 
 // Codeword of row i / column j of job J: A*i for the codeword progression, the
-// lattice codeword for grid rows and (2-D) columns.
+// lattice codeword for grid rows and (2-D) columns, the extended Hamming
+// codeword for the all-pairs Hamming jobs.
 __device__ __forceinline__ uint64_t mma_row_value(const Job* J, uint64_t i) {
-  return __ldg(&J->row_kind) == ROW_LATTICE ? lattice_value(__ldg(&J->A), i, __ldg(&J->row_step), __ldg(&J->t32))
-                                            : __ldg(&J->A) * i;
+  switch (__ldg(&J->row_kind)) {
+    case ROW_LATTICE: return lattice_value(__ldg(&J->A), i, __ldg(&J->row_step), __ldg(&J->t32));
+    case ROW_HAMMING_EXT: return hamming_cw_ext(i, __ldg(&J->n));
+    default: return __ldg(&J->A) * i;
+  }
 }
 __device__ __forceinline__ uint64_t mma_col_value(const Job* J, uint64_t j) {
-  return __ldg(&J->col_kind) == COL_LATTICE ? lattice_value(__ldg(&J->A), j, __ldg(&J->col_step), __ldg(&J->t32))
-                                            : __ldg(&J->A) * j;
+  switch (__ldg(&J->col_kind)) {
+    case COL_LATTICE: return lattice_value(__ldg(&J->A), j, __ldg(&J->col_step), __ldg(&J->t32));
+    case COL_HAMMING_EXT: return hamming_cw_ext(j, __ldg(&J->n));
+    default: return __ldg(&J->A) * j;
+  }
 }
 
 struct Shared {
@@ -383,9 +390,15 @@ __global__ void __launch_bounds__(kThreads, 1) mma_hist_kernel(MmaArgs args) {
         full = (r0 + kM <= N) && (c0 + kSuper <= N) && sr != sc;
       }
       if (r0 >= N) continue;  // uniform over the group
-      // every codeword of the job lies below A * 2^n (lattice points are indices < 2^n)
-      const uint64_t maxcw = A * ((1ull << __ldg(&jp->n)) - 1ull);
-      int L = 64 - __clzll((long long)(maxcw | 1));
+      // every AN codeword of the job lies below A * 2^n (lattice points are indices
+      // < 2^n); an extended Hamming codeword has nbins - 1 bits
+      int L;
+      if (__ldg(&jp->row_kind) == ROW_HAMMING_EXT) {
+        L = (int)__ldg(&jp->nbins) - 1;
+      } else {
+        const uint64_t maxcw = A * ((1ull << __ldg(&jp->n)) - 1ull);
+        L = 64 - __clzll((long long)(maxcw | 1));
+      }
       L = (L + 3) & ~3;
       const uint32_t slot = (uint32_t)(s & 1);
       const bool need_b = jn != bjob || sc != bsc;
@@ -581,16 +594,21 @@ __global__ void __launch_bounds__(kThreads, 1) mma_hist_kernel(MmaArgs args) {
 // Bit planes of the operands of job j: the bits of A * (2^n - 1), which bounds
 // every codeword of the job, rounded up to 4 (the kernel computes the same).
 int mma_operand_bits(const Job& j) {
-  const unsigned __int128 maxcw = (unsigned __int128)j.A * ((1ull << j.n) - 1ull);
   int bits = 0;
-  for (unsigned __int128 v = maxcw; v; v >>= 1) ++bits;
-  if (bits == 0) bits = 1;
+  if (j.row_kind == ROW_HAMMING_EXT) {
+    bits = (int)j.nbins - 1;  // extended Hamming codeword: n data + h check bits
+  } else {
+    const unsigned __int128 maxcw = (unsigned __int128)j.A * ((1ull << j.n) - 1ull);
+    for (unsigned __int128 v = maxcw; v; v >>= 1) ++bits;
+    if (bits == 0) bits = 1;
+  }
   return (bits + 3) & ~3;
 }
 
 bool mma_eligible(const Job& j) {
   if (j.kind != JOB_PAIRS || j.n > 48) return false;
-  const bool tri = j.shape == SHAPE_TRIANGLE && j.row_kind == ROW_PROGRESSION && j.col_kind == COL_PROGRESSION;
+  const bool tri = j.shape == SHAPE_TRIANGLE && ((j.row_kind == ROW_PROGRESSION && j.col_kind == COL_PROGRESSION) ||
+                                                 (j.row_kind == ROW_HAMMING_EXT && j.col_kind == COL_HAMMING_EXT));
   const bool rect = j.shape == SHAPE_RECT && (j.row_kind == ROW_PROGRESSION || j.row_kind == ROW_LATTICE) &&
                     (j.col_kind == COL_PROGRESSION || j.col_kind == COL_LATTICE) && j.col_tiles * kSuper >= j.cols;
   return (tri || rect) && mma_operand_bits(j) <= 60;

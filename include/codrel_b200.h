@@ -64,8 +64,9 @@ typedef enum dd_mode {
   DD_MODE_MONTE_CARLO = 3  /* Philox4x32-10 sampled pairs (replaces cuRAND Sobol32) */
 } dd_mode;
 
-/* Which kernel family computes an AN exhaustive or grid histogram (Monte Carlo,
- * Ext-Hamming and anything wider than 60-bit operands use the popc kernel). */
+/* Which kernel family computes an AN exhaustive or grid histogram or an
+ * Ext-Hamming all-pairs brute force (Monte Carlo, the Ext-Hamming weight
+ * enumerator and anything wider than 60-bit operands use the popc kernel). */
 typedef enum dd_kernel {
   DD_KERNEL_AUTO = 0,  /* autotuner's choice for the shape */
   DD_KERNEL_POPC = 1,  /* XOR + POPC, warp-private shared-memory bins */

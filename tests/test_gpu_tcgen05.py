@@ -96,3 +96,32 @@ def test_mma_grid_archive(ctx):
         assert res.counts == x["counts"], x["file"]
         checked += 1
     assert checked >= 90
+
+
+# -- Ext-Hamming all-pairs brute force on the tcgen05 path --------------------------
+@pytest.mark.parametrize("n", [8, 16])
+@pytest.mark.parametrize("method", [dd.HAMMING_ALL_PAIRS, dd.HAMMING_ALL_PAIRS_DISTINCT])
+def test_mma_hamming_all_pairs(ctx, n, method):
+    for w1 in (0, 1):
+        kw = dict(with_1bit=w1, hamming_method=method)
+        a = ctx.histogram(dd.Request(dd.CODE_EXT_HAMMING, dd.MODE_EXHAUSTIVE, 1, n, kernel=dd.KERNEL_MMA, **kw))
+        b = ctx.histogram(dd.Request(dd.CODE_EXT_HAMMING, dd.MODE_EXHAUSTIVE, 1, n, kernel=dd.KERNEL_POPC, **kw))
+        assert a.kernel_used == dd.KERNEL_MMA and b.kernel_used == dd.KERNEL_POPC
+        assert a.raw == b.raw and a.counts == b.counts
+        if n == 8:
+            f = oracle.hamming_pairs_distinct_raw if method == dd.HAMMING_ALL_PAIRS_DISTINCT else oracle.hamming_pairs_raw
+            assert a.counts == f(n, w1, a.nbins)
+
+
+def test_mma_hamming_reference_runs(ctx):
+    """The reference's own `-e 2/3` stdout tables, on the tcgen05 path."""
+    method = {"2": dd.HAMMING_ALL_PAIRS, "3": dd.HAMMING_ALL_PAIRS_DISTINCT, "4": dd.HAMMING_ALL_PAIRS}
+    runs = [r for r in golden("ref_runs.json") if r["args"][0] == "-e" and r["args"][1] in method]
+    assert runs
+    for run in runs:
+        args = run["args"]
+        res = ctx.histogram(dd.Request(dd.CODE_EXT_HAMMING, dd.MODE_EXHAUSTIVE, 1, int(args[-1]),
+                                       with_1bit=int("-b" in args), hamming_method=method[args[1]],
+                                       kernel=dd.KERNEL_MMA))
+        assert res.kernel_used == dd.KERNEL_MMA
+        assert res.counts == run["counts"], args

@@ -178,7 +178,8 @@ static int plan_launch(dd_context* ctx, std::vector<Job>& jobs, const std::vecto
   lp.margs.status = status;
   lp.margs.timeout_ns = ctx->mma_timeout_ns;
   if (lp.nmma && tm) {
-    lp.msmem = mma_smem_bytes(lp.margs.hist_rows);
+    lp.margs.b_bufs = mma_b_bufs(lp.margs.hist_rows);
+    lp.msmem = mma_smem_bytes(lp.margs.hist_rows, lp.margs.b_bufs);
     lp.mgrid = (int)std::min<uint64_t>((uint64_t)ctx->num_sms, tm);  // one CTA (one TMEM owner) per SM
   }
   std::memcpy(ctx->h_jobs, table.data(), table.size() * sizeof(Job));

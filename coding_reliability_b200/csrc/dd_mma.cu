@@ -225,6 +225,7 @@ struct StripInfo {
   unsigned long long n;     // rows (codewords of a triangle job, lattice points of a grid job)
   unsigned long long cols;  // columns
   uint32_t job, flags;      // kInfoDone | kInfoFull | kInfoRect
+  uint32_t bbuf, pad;       // column-operand buffer the strip reads
 };
 
 // Codeword of row i / column j of job J: A*i for the codeword progression, the
@@ -310,10 +311,12 @@ __device__ __forceinline__ bool wait_or_abort(uint32_t addr, uint32_t parity, un
 // rows at or above the job's bin count are flagged at the flush.
 __global__ void __launch_bounds__(kThreads, 1) mma_hist_kernel(MmaArgs args) {
   extern __shared__ __align__(1024) uint8_t smem[];
-  uint8_t* sB = smem;                                        // 64 KB: 8 column tiles of one super tile
-  uint8_t* sA = smem + kBBytes;                              // 2 x 8 KB: row operand, double-buffered by strip
-  uint32_t* hist = reinterpret_cast<uint32_t*>(smem + kBBytes + 2 * kABytes);  // hist_rows x kEpiThreads
-  Shared* sh = reinterpret_cast<Shared*>(smem + kBBytes + 2 * kABytes + (size_t)args.hist_rows * kEpiThreads * 4);
+  // b_bufs x 64 KB: the column operand of a super tile (4 tiles of 256 columns), double-buffered
+  // when it fits, so the next super tile's operand is written while the current one's MMAs run
+  uint8_t* sB = smem;
+  uint8_t* sA = smem + (size_t)args.b_bufs * kBBytes;        // 2 x 8 KB: row operand, double-buffered by strip
+  uint32_t* hist = reinterpret_cast<uint32_t*>(sA + 2 * kABytes);  // hist_rows x kEpiThreads
+  Shared* sh = reinterpret_cast<Shared*>(sA + 2 * kABytes + (size_t)args.hist_rows * kEpiThreads * 4);
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   volatile uint32_t* abort = &sh->abort;
@@ -344,7 +347,8 @@ __global__ void __launch_bounds__(kThreads, 1) mma_hist_kernel(MmaArgs args) {
     const int gtid = tid - (kEpiThreads + 32);
     uint64_t s = 0;  // strips published
     uint32_t bjob = 0xffffffffu;
-    uint64_t bsc = ~0ull;  // column super tile whose operand is in sB
+    uint64_t bsc = ~0ull;  // column super tile whose operand is in buffer bcur
+    uint32_t bfill = 0, bcur = 0;  // column operands written so far, the buffer of the latest
     unsigned long long t = 0, end = 0;
     bool normal = false;
     for (;;) {
@@ -402,11 +406,13 @@ __global__ void __launch_bounds__(kThreads, 1) mma_hist_kernel(MmaArgs args) {
       L = (L + 3) & ~3;
       const uint32_t slot = (uint32_t)(s & 1);
       const bool need_b = jn != bjob || sc != bsc;
-      // the column operand may be rewritten once every MMA of strip s-1 is done,
-      // this slot's row operand once every MMA of strip s-2 is done
+      // this slot's row operand may be rewritten once every MMA of strip s-2 is
+      // done; a single column-operand buffer once every MMA of strip s-1 is done.
+      // With two buffers, the one rewritten was last read by strips up to s-2 (the
+      // other buffer serves at least strip s-1), so the s-2 wait covers it too.
       if (gtid == 0) {
         bool ok = true;
-        if (need_b && s >= 1)
+        if (need_b && args.b_bufs == 1 && s >= 1)
           ok = wait_or_abort(smem_u32(&sh->slot_free[(s - 1) & 1]), (uint32_t)((s - 1) >> 1) & 1u, args.timeout_ns,
                              abort);
         else if (s >= 2)
@@ -416,10 +422,13 @@ __global__ void __launch_bounds__(kThreads, 1) mma_hist_kernel(MmaArgs args) {
       gen_bar();
       if (!sh->gflag) break;
       if (need_b) {
+        bcur = args.b_bufs == 2 ? (bfill & 1u) : 0u;
+        ++bfill;
+        uint8_t* bb = sB + (size_t)bcur * kBBytes;
 #pragma unroll 1
         for (int cc = gtid; cc < kSuper; cc += kGenThreads) {
           const uint64_t j = c0 + cc;
-          write_operand(sB + (cc / kN) * kBTileBytes, cc % kN, j < (rect ? NC : N) ? mma_col_value(jp, j) : 0, L,
+          write_operand(bb + (cc / kN) * kBTileBytes, cc % kN, j < (rect ? NC : N) ? mma_col_value(jp, j) : 0, L,
                         false);
         }
         bjob = jn;
@@ -441,6 +450,7 @@ __global__ void __launch_bounds__(kThreads, 1) mma_hist_kernel(MmaArgs args) {
         si.cols = rect ? NC : N;
         si.job = jn;
         si.flags = (full ? kInfoFull : 0u) | (rect ? kInfoRect : 0u);
+        si.bbuf = bcur;
         mbar_arrive(smem_u32(&sh->slot_full[slot]));
       }
       ++s;
@@ -481,7 +491,7 @@ __global__ void __launch_bounds__(kThreads, 1) mma_hist_kernel(MmaArgs args) {
           }
           tc_fence_after();
           const uint32_t d = tmem + b * (uint32_t)kN;
-          const uint32_t b0 = smem_u32(sB + tile * kBTileBytes);
+          const uint32_t b0 = smem_u32(sB + (size_t)si.bbuf * kBBytes + tile * kBTileBytes);
 #pragma unroll
           for (int ks = 0; ks < kK / 32; ++ks)  // K = 32 bytes per instruction = 2 core matrices
             mma_i8(d, smem_desc(a0 + ks * 2 * kLBO), smem_desc(b0 + ks * 2 * kLBO), ks > 0 ? 1u : 0u);
@@ -614,9 +624,17 @@ bool mma_eligible(const Job& j) {
   return (tri || rect) && mma_operand_bits(j) <= 60;
 }
 
-size_t mma_smem_bytes(uint32_t hist_rows) {
-  size_t s = (size_t)2 * kABytes + kBBytes + (size_t)hist_rows * kEpiThreads * 4 + sizeof(Shared) + 64;
+size_t mma_smem_bytes(uint32_t hist_rows, uint32_t b_bufs) {
+  size_t s = (size_t)2 * kABytes + (size_t)b_bufs * kBBytes + (size_t)hist_rows * kEpiThreads * 4 + sizeof(Shared) + 64;
   return s < kMinSmem ? kMinSmem : s;
+}
+
+uint32_t mma_b_bufs(uint32_t hist_rows) {
+  int dev = 0, optin = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess)
+    return 1;
+  return mma_smem_bytes(hist_rows, 2) <= (size_t)optin ? 2u : 1u;
 }
 
 cudaError_t launch_mma(const MmaArgs& args, int grid, size_t smem, cudaStream_t stream) {

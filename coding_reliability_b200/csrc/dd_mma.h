@@ -16,13 +16,17 @@ struct MmaArgs {
   unsigned long long* counter;
   unsigned* status;          // KSTATUS_* bits, zeroed before the launch
   unsigned long long timeout_ns;  // bound of every mbarrier wait
+  uint32_t b_bufs;           // column-operand buffers in shared memory: 2 when they fit next to the bins, else 1
+  uint32_t pad;
 };
 
 // True if the job can run on the MMA path (AN exhaustive, codewords <= 60 bits).
 bool mma_eligible(const Job& j);
 // Operand bit planes L of job j; its distances lie in [0, L].
 int mma_operand_bits(const Job& j);
-size_t mma_smem_bytes(uint32_t hist_rows);
+// Column-operand buffers that fit in shared memory next to hist_rows bin rows.
+uint32_t mma_b_bufs(uint32_t hist_rows);
+size_t mma_smem_bytes(uint32_t hist_rows, uint32_t b_bufs);
 cudaError_t launch_mma(const MmaArgs& args, int grid, size_t smem, cudaStream_t stream);
 
 }  // namespace dd

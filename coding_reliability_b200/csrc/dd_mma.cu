@@ -62,6 +62,15 @@ constexpr uint32_t kMinSmem = 120 * 1024;  // more than half an SM: one CTA (and
 // fixed, independent of MmaArgs::timeout_ns (which a caller may set very short).
 constexpr unsigned long long kDrainTimeoutNs = 2000000000ull;
 constexpr int kBufs = kTmemCols / kN;   // accumulator buffers
+// Pauses (ns) between the polls of a waiting epilogue warp (for its next tile),
+// of the issuer (for a free accumulator buffer) and of the generators (for a free
+// operand slot).  A poll is a shared-memory pipe operation, as is every binning
+// atomic: 400 ns for the epilogue measured best (k=22: 5.96e12 pairs/s without a
+// pause, 6.09e12 at 120 ns, 6.14e12 at 400 ns, 6.03e12 at 1000 ns); a pause for
+// the issuer changed nothing.
+constexpr unsigned kEpiPollNs = 400;
+constexpr unsigned kIssuerPollNs = 0;
+constexpr unsigned kGenPollNs = 0;
 constexpr int kColsPerWarp = kN / (kEpiWarps / 4);  // columns of a tile each epilogue warp reads
 constexpr int kLoads = kColsPerWarp / 32;           // 32-column TMEM loads per warp and tile
 static_assert(kEpiWarps % 4 == 0 && kColsPerWarp % 32 == 0, "whole 32-column TMEM loads per warp and tile");
@@ -273,13 +282,16 @@ __device__ __forceinline__ void mbar_arrive(uint32_t addr) {
 
 // Bounded wait (single thread): true when the phase completed; false after
 // timeout_ns or once another thread has aborted (then this one aborts too).
-// The abort flag (shared memory) and the timer are checked every 32 polls: the
-// polls themselves go through the shared-memory pipe the epilogue's atomics load.
+// The abort flag (shared memory) and the timer are checked every 32 polls.  The
+// polls go through the shared-memory pipe that the epilogue's atomics load, so a
+// waiter may pause kSleepNs between polls to leave that pipe to the binning warps.
+template <unsigned kSleepNs = 0>
 __device__ __forceinline__ bool wait_or_abort(uint32_t addr, uint32_t parity, unsigned long long timeout_ns,
                                               volatile uint32_t* abort) {
   if (mbar_try_wait(addr, parity)) return true;
   const uint64_t t0 = globaltimer();
   for (uint32_t spin = 1;; ++spin) {
+    if constexpr (kSleepNs > 0) __nanosleep(kSleepNs);
     if (mbar_try_wait(addr, parity)) return true;
     if ((spin & 31) == 0) {
       if (*abort) return false;
@@ -413,10 +425,11 @@ __global__ void __launch_bounds__(kThreads, 1) mma_hist_kernel(MmaArgs args) {
       if (gtid == 0) {
         bool ok = true;
         if (need_b && args.b_bufs == 1 && s >= 1)
-          ok = wait_or_abort(smem_u32(&sh->slot_free[(s - 1) & 1]), (uint32_t)((s - 1) >> 1) & 1u, args.timeout_ns,
-                             abort);
+          ok = wait_or_abort<kGenPollNs>(smem_u32(&sh->slot_free[(s - 1) & 1]), (uint32_t)((s - 1) >> 1) & 1u,
+                                         args.timeout_ns, abort);
         else if (s >= 2)
-          ok = wait_or_abort(smem_u32(&sh->slot_free[slot]), (uint32_t)((s - 2) >> 1) & 1u, args.timeout_ns, abort);
+          ok = wait_or_abort<kGenPollNs>(smem_u32(&sh->slot_free[slot]), (uint32_t)((s - 2) >> 1) & 1u,
+                                         args.timeout_ns, abort);
         sh->gflag = ok ? 1u : 0u;
       }
       gen_bar();
@@ -471,7 +484,8 @@ __global__ void __launch_bounds__(kThreads, 1) mma_hist_kernel(MmaArgs args) {
       // until the epilogue has read tile gg-4, the previous tile of gg's buffer
       auto wait_empty = [&](uint64_t gg) -> bool {
         return gg < kBufs ||
-               wait_or_abort(smem_u32(&sh->empty[buf_of(gg)]), parity_of(gg - kBufs), args.timeout_ns, abort);
+               wait_or_abort<kIssuerPollNs>(smem_u32(&sh->empty[buf_of(gg)]), parity_of(gg - kBufs), args.timeout_ns,
+                                            abort);
       };
       for (uint64_t s = 0;; ++s) {
         const uint32_t slot = (uint32_t)(s & 1);
@@ -538,7 +552,7 @@ __global__ void __launch_bounds__(kThreads, 1) mma_hist_kernel(MmaArgs args) {
     for (uint64_t g = 0;; ++g) {
       const uint32_t b = buf_of(g);
       bool r = true;
-      if (lane == 0) r = wait_or_abort(smem_u32(&sh->full[b]), parity_of(g), args.timeout_ns, abort);
+      if (lane == 0) r = wait_or_abort<kEpiPollNs>(smem_u32(&sh->full[b]), parity_of(g), args.timeout_ns, abort);
       if (!__shfl_sync(0xffffffffu, r ? 1 : 0, 0)) { ok = false; break; }
       __syncwarp();  // lane 0's wait acquired the MMA result (and StripInfo); this orders it for the warp
       const uint32_t tile = (uint32_t)(g % kTilesPerStrip);

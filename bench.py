@@ -38,7 +38,7 @@ sys.path.insert(0, str(ROOT))
 
 METRIC = "exact pairs/s (AN k=24 exhaustive histogram)"
 NCU_DRAM_BYTES_PER_LAUNCH = 108288  # popc path, measured by ncu (see profiles/)
-NCU_DRAM_BYTES_PER_LAUNCH_MMA = 113664  # tcgen05 path, measured by ncu (see profiles/)
+NCU_DRAM_BYTES_PER_LAUNCH_MMA = 81408  # tcgen05 path, measured by ncu (see profiles/)
 UNIT = "pairs/s"
 
 

@@ -270,7 +270,11 @@ struct Shared {
   uint32_t abort;         // set by whichever wait ran out; every other wait then gives up too
   uint32_t gflag;         // generators: result of their thread 0's wait
   uint32_t pad;
-  unsigned long long gclaim;  // generators: first strip of the current claim
+  // generators: first strip of claim c in gclaim[c & 1].  Thread 0 rewrites an entry
+  // two claims later, past the barrier of the claim in between, which every thread
+  // reaches only after reading the entry (a single word could be overwritten first
+  // when every strip of a claim is skipped)
+  unsigned long long gclaim[2];
 };
 
 // Barrier 1 over the generator warps only (barrier 0 is __syncthreads).
@@ -361,13 +365,15 @@ __global__ void __launch_bounds__(kThreads, 1) mma_hist_kernel(MmaArgs args) {
     uint32_t bjob = 0xffffffffu;
     uint64_t bsc = ~0ull;  // column super tile whose operand is in buffer bcur
     uint32_t bfill = 0, bcur = 0;  // column operands written so far, the buffer of the latest
+    uint32_t nclaim = 0;           // claims taken
     unsigned long long t = 0, end = 0;
     bool normal = false;
     for (;;) {
       if (t >= end) {
-        if (gtid == 0) sh->gclaim = atomicAdd(args.counter, (unsigned long long)kStrips);
+        if (gtid == 0) sh->gclaim[nclaim & 1] = atomicAdd(args.counter, (unsigned long long)kStrips);
         gen_bar();
-        const unsigned long long base = sh->gclaim;
+        const unsigned long long base = sh->gclaim[nclaim & 1];
+        ++nclaim;
         if (base >= args.total_tiles) { normal = true; break; }
         t = base;
         end = base + kStrips < args.total_tiles ? base + (unsigned long long)kStrips

@@ -39,6 +39,9 @@ sys.path.insert(0, str(ROOT))
 METRIC = "exact pairs/s (AN k=24 exhaustive histogram)"
 NCU_DRAM_BYTES_PER_LAUNCH = 108288  # popc path, measured by ncu (see profiles/)
 NCU_DRAM_BYTES_PER_LAUNCH_MMA = 81408  # tcgen05 path, measured by ncu (see profiles/)
+NCU_TENSOR_PIPE_PCT_MMA = 16.9  # sm__pipe_tensor_cycles_active of the same capture
+INT8_DENSE_TOPS_NOMINAL = 4500.0  # B200 dense int8 tensor rate (nominal; the driver measures bf16 only)
+MMA_K_PAD = 64  # int8 K of every tcgen05 tile (operand bit planes padded to 64)
 UNIT = "pairs/s"
 
 
@@ -266,7 +269,12 @@ def main() -> None:
                                       "on chip, so the figure does not grow with k",
                     "peak_source": "measured live: conflict-free red.shared.add loop, 16 warps per SM "
                                    "(dd_measure_red_peak)",
-                    "popc_path_equivalent_frac": per_gpu / popc_peak}
+                    "popc_path_equivalent_frac": per_gpu / popc_peak,
+                    # the tensor pipe beside it: 2 * K int8 operations per pair
+                    "tensor_pipe": {"achieved_tops": per_gpu * 2 * MMA_K_PAD / 1e12,
+                                    "peak_tops": INT8_DENSE_TOPS_NOMINAL, "peak_source": "nominal dense int8",
+                                    "frac": per_gpu * 2 * MMA_K_PAD / 1e12 / INT8_DENSE_TOPS_NOMINAL,
+                                    "ncu_tensor_cycles_active_pct": NCU_TENSOR_PIPE_PCT_MMA}}
     else:
         achieved_popc = per_gpu * 1.0  # one 32-bit POPC per pair (high word folded per segment)
         roofline = {"bound": "popc", "achieved": achieved_popc / 1e9, "peak": popc_peak / 1e9, "unit": "Gpopc/s",

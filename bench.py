@@ -30,6 +30,7 @@ import re
 import statistics
 import subprocess
 import sys
+import tempfile
 import time
 from pathlib import Path
 
@@ -40,7 +41,7 @@ METRIC = "exact pairs/s (AN k=24 exhaustive histogram)"
 NCU_DRAM_BYTES_PER_LAUNCH = 108288  # popc path, measured by ncu (see profiles/)
 NCU_DRAM_BYTES_PER_LAUNCH_MMA = 81408  # tcgen05 path, measured by ncu (see profiles/)
 NCU_TENSOR_PIPE_PCT_MMA = 16.9  # sm__pipe_tensor_cycles_active of the same capture
-INT8_DENSE_TOPS_NOMINAL = 4500.0  # B200 dense int8 tensor rate (nominal; the driver measures bf16 only)
+INT8_DENSE_TOPS_NOMINAL = 4500.0  # B200 dense int8 tensor rate (nominal; the measured peaks cover bf16 only)
 MMA_K_PAD = 64  # int8 K of every tcgen05 tile (operand bit planes padded to 64)
 UNIT = "pairs/s"
 
@@ -55,6 +56,8 @@ def parse():
     p.add_argument("--kernel", default="auto", choices=["auto", "popc", "mma"])
     p.add_argument("--no-extras", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--clocks-dir", default=os.environ.get("DD_CLOCKS_DIR", ""),
+                   help="folder for the nvidia-smi clock samples of the timed region (default: temp dir)")
     return p.parse_args()
 
 
@@ -235,8 +238,8 @@ def main() -> None:
     popc_peak = ctx.popc_peak()  # popc/s, measured on this GPU now
     red_peak = ctx.red_peak()    # shared-memory atomic adds/s, measured on this GPU now
 
-    clocks = ClockSampler(local, ROOT / "gpurun_out" / f"clocks_rank{rank}.csv") if \
-        (ROOT / "gpurun_out").exists() else ClockSampler(local, Path(f"/tmp/clocks_rank{rank}.csv"))
+    clocks_dir = Path(args.clocks_dir) if args.clocks_dir else Path(tempfile.gettempdir())
+    clocks = ClockSampler(local, clocks_dir / f"clocks_rank{rank}.csv")
     barrier()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     ev0.record(stream)

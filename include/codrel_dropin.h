@@ -6,10 +6,10 @@
  *   distance_distribution/src/algorithms.h:20-34   (main tool)
  *   distance_distribution_super_a/src/algorithms.h:20-21 (super-A fork)
  *
- * Differences a caller can observe are listed in DESIGN.md; in short: every
- * histogram is computed on one GPU (the `_cpu*` entry points keep their file
- * prefixes and conventions but do not run on the CPU), errors are reported by
- * exception instead of exit(), and Monte Carlo draws come from Philox4x32-10.
+ * Differences a caller can observe: every histogram is computed on one GPU
+ * (the `_cpu*` entry points keep their file prefixes and conventions but do
+ * not run on the CPU), errors are reported by exception instead of exit(), and
+ * Monte Carlo draws come from Philox4x32-10.
  */
 #ifndef CODREL_DROPIN_H_
 #define CODREL_DROPIN_H_

@@ -112,22 +112,6 @@ __device__ __forceinline__ uint64_t col_value(const Job& J, uint64_t j) {
   }
 }
 
-// Upper-triangle decode: s in [0, M(M+1)/2) -> (r, c), r <= c, row-major.
-__device__ __forceinline__ void tri_decode(uint64_t s, uint64_t M, uint64_t& r, uint64_t& c) {
-  const double b = 2.0 * (double)M + 1.0;
-  double disc = b * b - 8.0 * (double)s;
-  if (disc < 0) disc = 0;
-  int64_t rr = (int64_t)((b - sqrt(disc)) * 0.5);
-  if (rr < 0) rr = 0;
-  if ((uint64_t)rr >= M) rr = (int64_t)M - 1;
-  auto S = [M](uint64_t r_) { return r_ * M - (r_ * (r_ - (r_ ? 1 : 0))) / 2; };
-  // S(r) = r*M - r*(r-1)/2 entries precede row r
-  while ((uint64_t)rr + 1 < M && S((uint64_t)rr + 1) <= s) ++rr;
-  while (rr > 0 && S((uint64_t)rr) > s) --rr;
-  r = (uint64_t)rr;
-  c = r + (s - S(r));
-}
-
 // ---------------------------------------------------------------------------
 // pair tiles
 // ---------------------------------------------------------------------------

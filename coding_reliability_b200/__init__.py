@@ -14,6 +14,7 @@ from __future__ import annotations
 
 import ctypes as C
 import os
+import threading
 from dataclasses import dataclass, field
 from pathlib import Path
 
@@ -181,6 +182,7 @@ def load() -> C.CDLL:
     lib.dd_server_wait.argtypes = [vp, C.c_uint64, C.c_double, C.POINTER(_Res)]
     lib.dd_server_cancel.argtypes = [vp, C.c_uint64]
     lib.dd_server_get_stats.argtypes = [vp, C.c_void_p]
+    lib.dd_server_shutdown.argtypes = [vp]
     lib.dd_server_destroy.argtypes = [vp]
     _lib = lib
     return lib
@@ -359,39 +361,88 @@ class Server:
         opts = _ServerOpts(memory_budget_bytes, max_queue, round_ms, int(dry_run), int(inject_alloc_failure))
         _check(lib.dd_server_create(device, C.byref(opts), C.byref(h)))
         self._h = h
+        # calls in flight: close() frees the server only after they have returned
+        self._cv = threading.Condition()
+        self._users = 0
+        self._closing = False
+
+    def _enter(self):
+        with self._cv:
+            if self._closing or not self._h:
+                raise DDError(9, "server closed")
+            self._users += 1
+            return self._h
+
+    def _leave(self):
+        with self._cv:
+            self._users -= 1
+            self._cv.notify_all()
 
     def submit(self, req: Request) -> int:
         t = C.c_uint64()
-        _check(load().dd_server_submit(self._h, C.byref(req._c()), C.byref(t)))
+        h = self._enter()
+        try:
+            _check(load().dd_server_submit(h, C.byref(req._c()), C.byref(t)))
+        finally:
+            self._leave()
         return t.value
 
     def poll(self, ticket: int) -> Result | None:
         out, done = _Res(), C.c_int()
-        _check(load().dd_server_poll(self._h, ticket, C.byref(out), C.byref(done)))
+        h = self._enter()
+        try:
+            _check(load().dd_server_poll(h, ticket, C.byref(out), C.byref(done)))
+        finally:
+            self._leave()
         return Result._from(out) if done.value else None
 
     def wait(self, ticket: int, timeout_s: float = -1.0) -> tuple[int, Result]:
-        """(status, result): status is the query's dd_status (0 = done)."""
+        """(status, result): status is the query's dd_status (0 = done; 9 = cancelled,
+        also when the server is closed while this call waits)."""
         out = _Res()
-        st = load().dd_server_wait(self._h, ticket, timeout_s, C.byref(out))
+        h = self._enter()
+        try:
+            st = load().dd_server_wait(h, ticket, timeout_s, C.byref(out))
+        finally:
+            self._leave()
         if st in (7, 8):  # timeout / unknown ticket
             _check(st)
         return st, Result._from(out)
 
     def cancel(self, ticket: int) -> None:
-        _check(load().dd_server_cancel(self._h, ticket))
+        h = self._enter()
+        try:
+            _check(load().dd_server_cancel(h, ticket))
+        finally:
+            self._leave()
 
     def stats(self) -> dict:
         s = _ServerStats()
-        _check(load().dd_server_get_stats(self._h, C.byref(s)))
+        h = self._enter()
+        try:
+            _check(load().dd_server_get_stats(h, C.byref(s)))
+        finally:
+            self._leave()
         d = {k: getattr(s, k) for k, _ in _ServerStats._fields_}
         d["pairs"] = (d.pop("pairs_hi") << 64) | d.pop("pairs_lo")
         return d
 
     def close(self) -> None:
-        if getattr(self, "_h", None):
-            load().dd_server_destroy(self._h)
-            self._h = None
+        """Cancels unfinished queries (their waiters return status 9), waits for the
+        calls in flight, then frees the server.  Calls made afterwards raise DDError."""
+        cv = getattr(self, "_cv", None)
+        if cv is None or not getattr(self, "_h", None):
+            return
+        with cv:
+            if self._closing:
+                return
+            self._closing = True
+        lib = load()
+        lib.dd_server_shutdown(self._h)  # wakes every waiter
+        with cv:
+            cv.wait_for(lambda: self._users == 0)
+        lib.dd_server_destroy(self._h)
+        self._h = None
 
     def __enter__(self):
         return self

@@ -69,7 +69,12 @@ struct dd_server {
   std::mutex mu;
   std::condition_variable cv_work, cv_done;
   std::thread worker;
+  std::mutex shutdown_mu;      // serialises dd_server_shutdown (the worker is joined once)
   bool stop = false;
+  // calls inside the API functions below; dd_server_destroy frees nothing until
+  // every one has left (a waiter woken by the shutdown still has to re-take mu)
+  int inside = 0;
+  std::condition_variable cv_idle;
   int failed = DD_OK;
   std::string failure;
   uint64_t next_ticket = 1;
@@ -82,6 +87,17 @@ struct dd_server {
 };
 
 namespace {
+
+// Marks an API call as inside the server; constructed and destroyed with s->mu held.
+struct Inside {
+  dd_server* s;
+  explicit Inside(dd_server* srv) : s(srv) { ++s->inside; }
+  ~Inside() {
+    if (--s->inside == 0) s->cv_idle.notify_all();
+  }
+  Inside(const Inside&) = delete;
+  Inside& operator=(const Inside&) = delete;
+};
 
 void finish(dd_server* s, Query& q, int status) {
   q.done = true;
@@ -256,6 +272,7 @@ int dd_server_submit(dd_server* s, const dd_request* req, uint64_t* ticket) {
   q.pairs = dd::planned_pairs(q.shape, *req);
   q.t_submit = now_ms();
   std::lock_guard<std::mutex> lk(s->mu);
+  Inside in(s);
   if (s->failed != DD_OK) { dd::set_error("server failed: " + s->failure); return s->failed; }
   if (s->stop) { dd::set_error("server is shutting down"); return DD_ERR_CANCELLED; }
   if (s->queue.size() >= s->opt.max_queue && s->free_slots.empty()) {
@@ -275,6 +292,7 @@ int dd_server_submit(dd_server* s, const dd_request* req, uint64_t* ticket) {
 int dd_server_poll(dd_server* s, uint64_t ticket, dd_result* res, int* done) {
   if (!s || !done) { dd::set_error("NULL argument"); return DD_ERR_INVALID_ARGUMENT; }
   std::lock_guard<std::mutex> lk(s->mu);
+  Inside in(s);
   auto it = s->queries.find(ticket);
   if (it == s->queries.end()) { dd::set_error("unknown ticket"); return DD_ERR_NOT_FOUND; }
   *done = it->second.done ? 1 : 0;
@@ -285,6 +303,7 @@ int dd_server_poll(dd_server* s, uint64_t ticket, dd_result* res, int* done) {
 int dd_server_wait(dd_server* s, uint64_t ticket, double timeout_s, dd_result* res) {
   if (!s) { dd::set_error("NULL argument"); return DD_ERR_INVALID_ARGUMENT; }
   std::unique_lock<std::mutex> lk(s->mu);
+  Inside in(s);
   auto it = s->queries.find(ticket);
   if (it == s->queries.end()) { dd::set_error("unknown ticket"); return DD_ERR_NOT_FOUND; }
   auto ready = [&] { return s->queries[ticket].done; };
@@ -300,6 +319,7 @@ int dd_server_wait(dd_server* s, uint64_t ticket, double timeout_s, dd_result* r
 int dd_server_cancel(dd_server* s, uint64_t ticket) {
   if (!s) { dd::set_error("NULL argument"); return DD_ERR_INVALID_ARGUMENT; }
   std::lock_guard<std::mutex> lk(s->mu);
+  Inside in(s);
   auto it = s->queries.find(ticket);
   if (it == s->queries.end()) { dd::set_error("unknown ticket"); return DD_ERR_NOT_FOUND; }
   Query& q = it->second;
@@ -316,6 +336,7 @@ int dd_server_cancel(dd_server* s, uint64_t ticket) {
 int dd_server_get_stats(dd_server* s, dd_server_stats* out) {
   if (!s || !out) { dd::set_error("NULL argument"); return DD_ERR_INVALID_ARGUMENT; }
   std::lock_guard<std::mutex> lk(s->mu);
+  Inside in(s);
   std::memset(out, 0, sizeof(*out));
   out->submitted = s->submitted;
   out->admitted = s->admitted;
@@ -344,14 +365,26 @@ int dd_server_get_stats(dd_server* s, dd_server_stats* out) {
   return DD_OK;
 }
 
-int dd_server_destroy(dd_server* s) {
+int dd_server_shutdown(dd_server* s) {
   if (!s) return DD_OK;
+  std::lock_guard<std::mutex> once(s->shutdown_mu);
   {
     std::lock_guard<std::mutex> lk(s->mu);
     s->stop = true;
   }
   s->cv_work.notify_all();
+  // the scheduler cancels every unfinished query on its way out, which wakes the waiters
   if (s->worker.joinable()) s->worker.join();
+  return DD_OK;
+}
+
+int dd_server_destroy(dd_server* s) {
+  if (!s) return DD_OK;
+  dd_server_shutdown(s);
+  {
+    std::unique_lock<std::mutex> lk(s->mu);
+    s->cv_idle.wait(lk, [s] { return s->inside == 0; });
+  }
   if (s->d_slots) cudaFree(s->d_slots);
   if (s->ctx) dd_context_destroy(s->ctx);
   delete s;

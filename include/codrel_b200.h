@@ -242,7 +242,12 @@ int dd_server_wait(dd_server* s, uint64_t ticket, double timeout_s, dd_result* r
  * the current round and frees its slot; its result status is DD_ERR_CANCELLED. */
 int dd_server_cancel(dd_server* s, uint64_t ticket);
 int dd_server_get_stats(dd_server* s, dd_server_stats* out);
-/* Stops the scheduler; unfinished queries end with DD_ERR_CANCELLED. */
+/* Stops the scheduler: unfinished queries end with DD_ERR_CANCELLED, which
+ * wakes every thread blocked in dd_server_wait; later submits are refused.  The
+ * handle stays valid (wait / poll / stats still answer) until dd_server_destroy. */
+int dd_server_shutdown(dd_server* s);
+/* dd_server_shutdown, then frees the server once every call still inside it
+ * (a waiter it woke) has returned.  No call may start after this one. */
 int dd_server_destroy(dd_server* s);
 
 /* --- host-only helpers (no device needed) ------------------------------- */

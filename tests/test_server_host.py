@@ -44,12 +44,20 @@ def test_malformed_requests_refused_at_submit(lib):
         assert s.stats()["submitted"] == 0
 
 
+def until(cond, timeout_s=10.0):
+    """Polls cond() until it holds (the scheduler thread runs on its own time)."""
+    end = time.monotonic() + timeout_s
+    while not cond():
+        assert time.monotonic() < end, "condition not reached"
+        time.sleep(0.002)
+
+
 def test_admission_by_slots_and_queue_bound(lib):
     # one slot, queue of two: the big query holds the slot, two wait, the rest are refused
     with dd.Server(dry_run=True, round_ms=5, memory_budget_bytes=1000, max_queue=2) as s:
         assert s.stats()["slots"] == 1
         t_big = s.submit(big())
-        time.sleep(0.05)  # admitted into the only slot
+        until(lambda: s.stats()["active"] == 1)  # admitted into the only slot
         waiting = [s.submit(small()) for _ in range(2)]
         with pytest.raises(dd.DDError) as e:
             s.submit(small())
@@ -65,7 +73,7 @@ def test_admission_by_slots_and_queue_bound(lib):
 def test_small_query_overtakes_a_big_one(lib):
     with dd.Server(dry_run=True, round_ms=2) as s:
         t_big = s.submit(big())
-        time.sleep(0.02)
+        until(lambda: s.stats()["active"] == 1)
         t_small = s.submit(small())
         assert s.wait(t_small, 5)[0] == 0
         assert s.poll(t_big) is None  # still running: both shared the rounds
@@ -76,7 +84,7 @@ def test_small_query_overtakes_a_big_one(lib):
 def test_cancel_queued_query(lib):
     with dd.Server(dry_run=True, round_ms=5, memory_budget_bytes=1000, max_queue=4) as s:
         t_big = s.submit(big())
-        time.sleep(0.02)
+        until(lambda: s.stats()["active"] == 1)
         t_q = s.submit(small())
         s.cancel(t_q)
         assert s.wait(t_q, 1)[0] == 9
@@ -98,16 +106,45 @@ def test_shutdown_cancels_pending(lib):
     results = {}
 
     def waiter(t):
-        results[t] = s.wait(t, 10)[0]
+        try:
+            results[t] = s.wait(t, 10)[0]
+        except dd.DDError as e:  # the wait began after close(): the server refuses it
+            results[t] = e.status
 
-    th = [threading.Thread(target=waiter, args=(t,)) for t in (t_big, t_q)]
+    th = [threading.Thread(target=waiter, args=(t,), daemon=True) for t in (t_big, t_q)]
     for x in th:
         x.start()
     time.sleep(0.05)
     s.close()
     for x in th:
-        x.join(5)
+        x.join(10)
     assert results == {t_big: 9, t_q: 9}
+    with pytest.raises(dd.DDError):
+        s.submit(small())
+
+
+def test_close_while_many_threads_wait(lib):
+    # waiters woken by the shutdown still hold the server: it is freed only after they return
+    for _ in range(20):
+        s = dd.Server(dry_run=True, round_ms=1, memory_budget_bytes=1000)
+        tickets = [s.submit(big())] + [s.submit(small()) for _ in range(3)]
+        results, th = [], []
+        for t in tickets:
+            for _ in range(4):
+                def waiter(t=t):
+                    try:
+                        results.append(s.wait(t, 10)[0])
+                    except dd.DDError as e:
+                        results.append(e.status)
+                th.append(threading.Thread(target=waiter, daemon=True))
+        for x in th:
+            x.start()
+        s.close()
+        for x in th:
+            x.join(10)
+        assert len(results) == len(th)
+        # the small queries may finish before the shutdown; nothing else may happen
+        assert set(results) <= {0, 9}
 
 
 def test_many_clients_latency_stats(lib):

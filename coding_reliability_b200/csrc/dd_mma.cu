@@ -1,4 +1,5 @@
-// dd_mma.cu — tcgen05 kind::i8 bit-plane MMA kernel for AN exhaustive jobs.
+// dd_mma.cu — tcgen05 kind::i8 bit-plane MMA kernel: AN exhaustive, 1-D / 2-D
+// grid and Ext-Hamming all-pairs jobs.
 //
 // The Hamming distance of two codewords x, y (bit planes b_x, b_y in {0,1}^L)
 // is d = popc(x) + popc(y) - 2<b_x, b_y>.  The operands put that whole
@@ -16,16 +17,19 @@
 // columns: the MMA of tile t+1 runs while the epilogue bins tile t.  (Four
 // buffers of N = 128 measured 17 % slower: every tile costs each epilogue warp
 // a barrier poll and an arrive through the shared-memory pipe that its atomics
-// saturate, so fewer, wider tiles win over deeper buffering.)  Generator warps claim 8 strips at a time (one super tile
-// when the job's tile range is aligned), so the column operand of a super tile
-// is written once for its 8 strips; the row operand is double-buffered by strip
-// and written while the previous strip's MMAs run.
+// saturate, so fewer, wider tiles win over deeper buffering.)  Generator warps
+// claim 8 strips at a time (one super tile when the job's tile range is
+// aligned) and write the column operand once per super tile, into the second
+// of two buffers when both fit beside the bins, so the next super tile's
+// operand is written while the current one's MMAs run; the row operand is
+// double-buffered by strip.
 // One CTA per SM (16 epilogue warps, 1 issuer warp, 3 generator warps, 512 TMEM
 // columns).
 //
 // The epilogue is bound by the shared-memory atomic rate (one red.shared per
-// pair; about 32 per clock per SM measured on B200 for TMEM-resident values),
-// twice the POPC issue rate (16 per clock per SM) that bounds the popc kernel.
+// pair; about 31 per clock per SM measured on B200), twice the POPC issue rate
+// (16 per clock per SM) that bounds the popc kernel.  A waiting epilogue warp
+// pauses between its barrier polls, which share that pipe with the atomics.
 //
 // Every mbarrier wait is bounded (MmaArgs::timeout_ns); on expiry the CTA
 // records KSTATUS_TIMEOUT, every other wait gives up, the last MMA drains

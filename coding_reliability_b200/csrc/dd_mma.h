@@ -1,4 +1,4 @@
-// dd_mma.h — the tcgen05 (5th-gen tensor core) path for AN exhaustive jobs.
+// dd_mma.h — the tcgen05 (5th-gen tensor core) path: AN exhaustive, grid and Ext-Hamming all-pairs jobs.
 #pragma once
 #include <cuda_runtime.h>
 #include <cstddef>
@@ -20,7 +20,9 @@ struct MmaArgs {
   uint32_t pad;
 };
 
-// True if the job can run on the MMA path (AN exhaustive, codewords <= 60 bits).
+// True if the job can run on the MMA path: all pairs of a codeword progression or
+// of the Ext-Hamming codewords, or a grid of lattice rows and progression / lattice
+// columns; at most 60 operand bits.
 bool mma_eligible(const Job& j);
 // Operand bit planes L of job j; its distances lie in [0, L].
 int mma_operand_bits(const Job& j);

@@ -13,6 +13,7 @@ post-processed uint128 counts[] as Python ints.
 from __future__ import annotations
 
 import ctypes as C
+import json
 import os
 import threading
 from dataclasses import dataclass, field
@@ -160,6 +161,8 @@ def load() -> C.CDLL:
     lib.dd_context_destroy.argtypes = [vp]
     lib.dd_histogram.argtypes = [vp, C.POINTER(_Req), C.POINTER(_Res)]
     lib.dd_histogram_plain.argtypes = [vp, C.POINTER(_Req), C.POINTER(_Res)]
+    lib.dd_histogram_part.argtypes = [vp, C.POINTER(_Req), C.c_uint64, C.c_uint64, C.POINTER(C.c_uint64), u32,
+                                      C.POINTER(C.c_double)]
     lib.dd_batch_run.argtypes = [vp, C.POINTER(_Req), u32, C.POINTER(_Res), C.POINTER(_BatchOpts)]
     lib.dd_request_shape.argtypes = [C.POINTER(_Req), C.POINTER(u32), C.POINTER(u32), C.POINTER(C.c_uint64)]
     lib.dd_postprocess.argtypes = [C.POINTER(_Req), C.POINTER(C.c_uint64), u32, C.POINTER(_Res)]
@@ -237,6 +240,44 @@ def philox4x32_10(ctr: tuple[int, int, int, int], key: tuple[int, int]) -> tuple
     return tuple(o)
 
 
+def _request_key(req: Request) -> dict:
+    return {k: getattr(req, k) for k in ("code", "mode", "A", "n", "h", "m", "m2", "seed", "with_1bit",
+                                         "hamming_method", "convention")}
+
+
+def run_resumable(ctx, req: Request, state_path: str | os.PathLike, chunk_tiles: int = 0) -> Result:
+    """One histogram computed in parts with a checkpoint after each: the state
+    file holds the request, the next tile and the raw bins so far (JSON, written
+    atomically), and a later call with the same request and file resumes where
+    the last one stopped.  The file is removed once the result is complete.
+    chunk_tiles = 0: about 64 parts.  `ctx` needs `histogram_part`."""
+    path = Path(state_path)
+    total = request_plan(req)["tiles"]
+    nb = request_shape(req)[0]
+    key = _request_key(req)
+    nxt, raw = 0, [0] * nb
+    if path.exists():
+        st = json.loads(path.read_text())
+        if st.get("request") != key or st.get("tiles") != total:
+            raise DDError(1, f"{path}: checkpoint of another request")
+        nxt, raw = int(st["next_tile"]), [int(x) for x in st["raw"]]
+        if not (0 <= nxt <= total and len(raw) == nb):
+            raise DDError(1, f"{path}: damaged checkpoint")
+    step = chunk_tiles if chunk_tiles > 0 else max(1, -(-total // 64))
+    while nxt < total:
+        cnt = min(step, total - nxt)
+        raw, _ = ctx.histogram_part(req, nxt, cnt, raw)
+        nxt += cnt
+        tmp = path.with_name(path.name + ".tmp")
+        tmp.write_text(json.dumps({"request": key, "tiles": total, "next_tile": nxt, "raw": raw}))
+        os.replace(tmp, path)
+    res = postprocess(req, raw)
+    res.user_tag = req.user_tag
+    if path.exists():
+        path.unlink()
+    return res
+
+
 class Context:
     """One device + one CUDA stream (dd_context)."""
 
@@ -276,6 +317,19 @@ class Context:
         out = _Res()
         _check(load().dd_mc_extend(self._h, C.byref(req._c()), it_done, raw, C.byref(out)))
         return Result._from(out)
+
+    def histogram_part(self, req: Request, tile_begin: int, tile_count: int,
+                       raw: list[int] | None = None) -> tuple[list[int], float]:
+        """dd_histogram_part: tiles [tile_begin, tile_begin + tile_count) of the
+        request's tile space (request_plan(req)["tiles"]) added to `raw`; returns
+        (raw, kernel_ms).  Disjoint parts covering the space sum to the full raw
+        histogram; postprocess(req, raw) gives the result."""
+        arr = (C.c_uint64 * MAX_BINS)(*([int(x) for x in (raw or [])] + [0] * (MAX_BINS - len(raw or []))))
+        ms = C.c_double()
+        _check(load().dd_histogram_part(self._h, C.byref(req._c()), tile_begin, tile_count, arr, MAX_BINS,
+                                        C.byref(ms)))
+        nb = request_shape(req)[0]
+        return [int(arr[b]) for b in range(nb)], ms.value
 
     def histogram_plain(self, req: Request) -> Result:
         """The plain one-launch-per-instance baseline (AN exhaustive only)."""

@@ -602,6 +602,48 @@ int dd_mc_extend(dd_context* ctx, const dd_request* req, uint64_t it_done, const
   return run_requests(ctx, req, 1, res, false, &c);
 }
 
+int dd_histogram_part(dd_context* ctx, const dd_request* req, uint64_t tile_begin, uint64_t tile_count,
+                      uint64_t* raw, uint32_t nraw, double* kernel_ms) {
+  if (!ctx || !req || !raw) { set_error("NULL argument"); return DD_ERR_INVALID_ARGUMENT; }
+  if (kernel_ms) *kernel_ms = 0.0;
+  Shape s;
+  std::string err;
+  int st = derive_shape(*req, s, err);
+  if (st != DD_OK) { set_error(err); return st; }
+  if (nraw < s.nbins) { set_error("raw histogram shorter than n+h+1"); return DD_ERR_INVALID_ARGUMENT; }
+  std::vector<Job> jobs;
+  plan_jobs(s, *req, jobs);
+  Job& j = jobs[0];
+  if (tile_begin > j.tiles || tile_count > j.tiles - tile_begin) {
+    set_error("tile range outside the request's tile space (dd_request_plan gives its size)");
+    return DD_ERR_INVALID_ARGUMENT;
+  }
+  if (tile_count == 0) return DD_OK;
+  // the kernel choice follows dd_histogram's (the autotuner's verdict for AUTO)
+  if (!ctx->tuned && req->kernel == DD_KERNEL_AUTO && req->code == DD_CODE_AN && req->mode == DD_MODE_EXHAUSTIVE &&
+      req->n >= 20) {
+    st = dd_autotune(ctx, nullptr);
+    if (st != DD_OK) return st;
+  }
+  st = ensure_capacity(ctx, 1, 1);
+  if (st != DD_OK) return st;
+  // the sub-range runs exactly as a query server round runs a query's share
+  j.tile_offset = tile_begin;
+  j.tiles = tile_count;
+  j.bins = ctx->d_bins;
+  DD_CUDA(cudaMemsetAsync(ctx->d_bins, 0, kMaxBins * sizeof(unsigned long long), ctx->stream));
+  const std::vector<uint32_t> kernels{req->kernel};
+  float ms = 0.0f;
+  st = launch_round(ctx, jobs, kernels, &ms);
+  if (st != DD_OK) return st;
+  DD_CUDA(cudaMemcpyAsync(ctx->h_bins, ctx->d_bins, kMaxBins * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                          ctx->stream));
+  DD_CUDA(cudaStreamSynchronize(ctx->stream));
+  for (uint32_t b = 0; b < s.nbins; ++b) raw[b] += ctx->h_bins[b];
+  if (kernel_ms) *kernel_ms = ms;
+  return DD_OK;
+}
+
 int dd_histogram_plain(dd_context* ctx, const dd_request* req, dd_result* res) {
   if (!ctx || !req || !res) { set_error("NULL argument"); return DD_ERR_INVALID_ARGUMENT; }
   if (req->code != DD_CODE_AN || req->mode != DD_MODE_EXHAUSTIVE) {

@@ -154,6 +154,18 @@ int dd_context_destroy(dd_context* ctx);
  * super-A run_ancoding (super_a/src/an_coding.cu:135). */
 int dd_histogram(dd_context* ctx, const dd_request* req, dd_result* res);
 
+/* One part of a request's work: the tiles [tile_begin, tile_begin + tile_count)
+ * of its tile space (dd_request_plan's `tiles`), computed on the context's GPU
+ * and ADDED to raw[0 .. n+h+1) (nraw >= n+h+1).  Disjoint parts that cover the
+ * tile space sum to the raw histogram of dd_histogram, bit for bit, whatever
+ * their sizes, order, kernels or GPUs; dd_postprocess turns the sum into the
+ * result.  So a long run can stop between parts and resume from (next tile,
+ * raw) - the state the reference keeps in one kernel launch of up to hours
+ * (src/an_coding.cu:243-282) - and one instance can be split over GPUs with
+ * a host-side sum.  kernel_ms (may be NULL): device time of the part. */
+int dd_histogram_part(dd_context* ctx, const dd_request* req, uint64_t tile_begin, uint64_t tile_count,
+                      uint64_t* raw, uint32_t nraw, double* kernel_ms);
+
 /* The plain one-launch-per-instance baseline for AN exhaustive requests: the
  * reference's design on this GPU (src/an_coding.cu:50-105 + :276-421): bins
  * allocated and freed per call, a grid-stride kernel of 128 CTAs per SM with

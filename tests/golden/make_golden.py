@@ -7,6 +7,8 @@ default /root/reference):
   * distance_distribution/results/{GridMs,converge/geom,runtimes/0,As}/*grid1d*.csv
                                                    1-D grid histograms (A=61 and others)
   * distance_distribution/results/superAs/*.txt    super-A sweep minima
+  * distance_distribution/results/converge/{pseudo,sobol,sobolSinus}/*.csv
+                                                   the reference's Monte Carlo runs (A=61)
   * the reference's own tool built from its sources (oracle/_ref/ref_codrel):
     full stdout of CPU-path runs, used for the results-file layout and counts.
   * the reference's ANcandidates tool built from its source
@@ -90,6 +92,20 @@ def an_grid() -> list:
     return out
 
 
+def an_mc_converge() -> list:
+    """The reference's Monte Carlo runs (cuRAND pseudo-random, Sobol and
+    scrambled-Sobol draws) of A=61, n=16/24 at many sample counts; the draws
+    cannot be replayed, so these pin the Monte Carlo path statistically."""
+    out = []
+    for kind in ("pseudo", "sobol", "sobolSinus"):
+        for p in sorted((RES / "converge" / kind).glob("ancoding_mc_gpu_m*_A*_n*_h*.csv")):
+            m = re.match(r"ancoding_mc_gpu_m(\d+)_A(\d+)_n(\d+)_h(\d+)\.csv", p.name)
+            out.append({"file": str(p.relative_to(RES.parent)), "kind": kind, "m": int(m.group(1)),
+                        "A": int(m.group(2)), "n": int(m.group(3)), "h": int(m.group(4)),
+                        "counts": parse_counts(p)})
+    return out
+
+
 def super_a() -> list:
     out = []
     for p in sorted((RES / "superAs").glob("superA_n*_h*.txt")):
@@ -165,6 +181,7 @@ FIXTURES = {
     "solutions.json": solutions,
     "an_exhaustive.json": an_exhaustive,
     "an_grid1d.json": an_grid,
+    "an_mc_converge.json": an_mc_converge,
     "super_a.json": super_a,
     "ref_runs.json": ref_runs,
     "ancandidates.json": ancandidates,

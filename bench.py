@@ -7,7 +7,11 @@ A=58659 (16-bit odd constant), k=24 data bits: 40-bit codewords, all
 One step = one full histogram through the C-ABI (dd_histogram).
 
 Also measured (extra keys): the k=16 256-candidate super-A sweep as ONE
-batched, graph-captured launch vs 256 plain one-launch-per-instance calls.
+batched, graph-captured launch vs 256 one-launch-per-instance calls of the
+persistent kernels and vs 256 plain one-launch-per-instance calls; the query
+server on the seeded serving mix; the candidate pre-filter.  Outside the timed
+region the headline histogram is computed once more on the other kernel and
+must be identical (`parity`).
 
 Reported per the harness contract: one JSON line on rank 0.
   value   pairs/s from the kernel's own CUDA events (codewords are generated
@@ -38,8 +42,8 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 METRIC = "exact pairs/s (AN k=24 exhaustive histogram)"
-NCU_DRAM_BYTES_PER_LAUNCH = 108288  # popc path, measured by ncu (see profiles/)
-NCU_DRAM_BYTES_PER_LAUNCH_MMA = 81408  # tcgen05 path, measured by ncu (see profiles/)
+NCU_DRAM_BYTES_PER_LAUNCH = 108288  # popc path: DRAM bytes of one launch, ncu capture at k=20
+NCU_DRAM_BYTES_PER_LAUNCH_MMA = 81408  # tcgen05 path: DRAM bytes of one launch, ncu capture at k=20
 NCU_TENSOR_PIPE_PCT_MMA = 16.9  # sm__pipe_tensor_cycles_active of the same capture
 INT8_DENSE_TOPS_NOMINAL = 4500.0  # B200 dense int8 tensor rate (nominal; the measured peaks cover bf16 only)
 MMA_K_PAD = 64  # int8 K of every tcgen05 tile (operand bit planes padded to 64)
@@ -56,6 +60,7 @@ def parse():
     p.add_argument("--kernel", default="auto", choices=["auto", "popc", "mma"])
     p.add_argument("--no-extras", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-parity", action="store_true", help="skip the cross-kernel check of the headline histogram")
     p.add_argument("--clocks-dir", default=os.environ.get("DD_CLOCKS_DIR", ""),
                    help="folder for the nvidia-smi clock samples of the timed region (default: temp dir)")
     return p.parse_args()
@@ -199,6 +204,26 @@ def replica_throughput(units_per_rank: int, world: int, slowest_ms: float) -> fl
     return units_per_rank * world / (slowest_ms * 1e-3)
 
 
+def counts_digest(counts: list[int]) -> str:
+    import hashlib
+    return hashlib.sha256(",".join(str(c) for c in counts).encode()).hexdigest()
+
+
+def cross_kernel_check(ctx, dd, A: int, k: int, timed) -> dict:
+    """Recomputes the timed histogram on the other kernel (popc <-> tcgen05)
+    and requires the identical raw bins and counts: two independent
+    implementations of the same exact histogram."""
+    other = dd.KERNEL_POPC if timed.kernel_used == dd.KERNEL_MMA else dd.KERNEL_MMA
+    o = ctx.histogram(dd.Request(dd.CODE_AN, dd.MODE_EXHAUSTIVE, A, k, kernel=other))
+    assert o.kernel_used == other
+    same = o.raw == timed.raw and o.counts == timed.counts
+    assert same, "the two kernels disagree on the headline histogram"
+    name = {dd.KERNEL_POPC: "popc", dd.KERNEL_MMA: "mma"}
+    return {"cross_kernel": same, "timed_kernel": name[timed.kernel_used], "other_kernel": name[other],
+            "other_kernel_pairs_per_s": pairs_of(k) / (o.kernel_ms * 1e-3),
+            "sha256_counts": counts_digest(timed.counts)}
+
+
 # ------------------------------------------------------------------------------------
 # the B200 arm
 # ------------------------------------------------------------------------------------
@@ -236,7 +261,9 @@ def main() -> None:
     for _ in range(args.warmup):
         ctx.histogram(req)
     popc_peak = ctx.popc_peak()  # popc/s, measured on this GPU now
-    red_peak = ctx.red_peak()    # shared-memory atomic adds/s, measured on this GPU now
+    red_sweep = ctx.red_sweep()  # shared-memory atomic adds/s at 8..32 warps per SM, both table layouts
+    red_best = max(red_sweep, key=lambda r: r["adds_per_s"])
+    red_peak = red_best["adds_per_s"]
 
     clocks_dir = Path(args.clocks_dir) if args.clocks_dir else Path(tempfile.gettempdir())
     clocks = ClockSampler(local, clocks_dir / f"clocks_rank{rank}.csv")
@@ -258,32 +285,48 @@ def main() -> None:
     assert all(r.counts == results[0].counts for r in results)
     assert sum(results[0].raw) == P
 
+    # the same histogram once more on the other kernel, outside the timed region
+    parity = None
+    if rank == 0 and not args.no_parity:
+        parity = cross_kernel_check(ctx, dd, A, k, results[0])
+
     value = replica_throughput(P * args.steps, world, t_kernel)
     e2e = replica_throughput(P * args.steps, world, t_total)
     per_gpu = P * args.steps / (kernel_ms * 1e-3)
     mma = results[0].kernel_used == dd.KERNEL_MMA
     if mma:
         # tcgen05 path: the tensor core computes the distances; the bound is the
-        # histogram epilogue's one shared-memory atomic per pair
-        roofline = {"bound": "shared_atomic", "achieved": per_gpu / 1e9, "peak": red_peak / 1e9, "unit": "Gred/s",
-                    "frac": per_gpu / red_peak, "traffic": NCU_DRAM_BYTES_PER_LAUNCH_MMA,
+        # histogram epilogue's shared-memory atomics: one per pair (single
+        # epilogue) or one per two pairs (paired epilogue, packed distance pairs)
+        paired = results[0].mma_epilogue == dd.MMA_EPILOGUE_PAIRED
+        apr = 0.5 if paired else 1.0
+        k_per_pair = MMA_K_PAD / (2 if paired else 1)  # int8 MACs per pair: one K=64 column per 2 or 1 pairs
+        per_pattern = {}
+        for r in red_sweep:
+            per_pattern[r["pattern"]] = max(per_pattern.get(r["pattern"], 0.0), r["adds_per_s"])
+        roofline = {"bound": "shared_atomic", "achieved": per_gpu * apr / 1e9, "peak": red_peak / 1e9,
+                    "unit": "Gred/s", "frac": per_gpu * apr / red_peak, "traffic": NCU_DRAM_BYTES_PER_LAUNCH_MMA,
                     "traffic_source": "dram__bytes_read.sum + dram__bytes_write.sum of one mma_hist_kernel launch, "
-                                      "ncu capture at k=20 (profiles/mma_hist_kernel_an_k20.md); operands are generated "
+                                      "ncu capture at k=20; operands are generated "
                                       "on chip, so the figure does not grow with k",
-                    "peak_source": "measured live: conflict-free red.shared.add loop, 16 warps per SM "
-                                   "(dd_measure_red_peak)",
+                    "epilogue": "paired" if paired else "single", "atomics_per_pair": apr,
+                    "pairs_per_s_at_peak": red_peak / apr,
+                    "peak_source": "measured live: maximum of a conflict-free red.shared.add sweep over 8..32 warps "
+                                   "per SM and two table layouts (dd_measure_red_sweep); best at "
+                                   f"{red_best['warps_per_sm']} warps, {red_best['pattern']}",
+                    "peak_by_layout_gred_s": {k: v / 1e9 for k, v in per_pattern.items()},
                     "popc_path_equivalent_frac": per_gpu / popc_peak,
-                    # the tensor pipe beside it: 2 * K int8 operations per pair
-                    "tensor_pipe": {"achieved_tops": per_gpu * 2 * MMA_K_PAD / 1e12,
+                    # the tensor pipe beside it: 2 * K int8 operations per MMA column
+                    "tensor_pipe": {"achieved_tops": per_gpu * 2 * k_per_pair / 1e12,
                                     "peak_tops": INT8_DENSE_TOPS_NOMINAL, "peak_source": "nominal dense int8",
-                                    "frac": per_gpu * 2 * MMA_K_PAD / 1e12 / INT8_DENSE_TOPS_NOMINAL,
+                                    "frac": per_gpu * 2 * k_per_pair / 1e12 / INT8_DENSE_TOPS_NOMINAL,
                                     "ncu_tensor_cycles_active_pct": NCU_TENSOR_PIPE_PCT_MMA}}
     else:
         achieved_popc = per_gpu * 1.0  # one 32-bit POPC per pair (high word folded per segment)
         roofline = {"bound": "popc", "achieved": achieved_popc / 1e9, "peak": popc_peak / 1e9, "unit": "Gpopc/s",
                     "frac": achieved_popc / popc_peak, "traffic": NCU_DRAM_BYTES_PER_LAUNCH,
                     "traffic_source": "dram__bytes_read.sum + dram__bytes_write.sum of one hist_kernel launch, "
-                                      "ncu capture at k=20 (profiles/hist_kernel_an_k20_popc.md); the kernel reads "
+                                      "ncu capture at k=20; the kernel reads "
                                       "only its job table and writes only its bins, so the figure does not grow with k",
                     "peak_source": "measured live: dependency-free POPC loop on this GPU (dd_measure_popc_peak)"}
     line = {
@@ -297,9 +340,11 @@ def main() -> None:
         "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": 256, "d2h_bytes_per_step": 64 * 8 * 8},
         "gpu_launches": args.steps,
         "clocks": clk,
-        "kernel_used": "mma" if mma else "popc",
+        "kernel_used": ("mma_" + dd.EPILOGUE_NAMES.get(results[0].mma_epilogue, "?")) if mma else "popc",
         "autotune": tuning,
     }
+    if parity is not None:
+        line["parity"] = parity
     if rank == 0 and not args.no_extras:
         line["super_a_sweep_k16"] = super_a_extra(ctx, dd)
         line["serving"] = serving_extra(dd)
@@ -314,12 +359,14 @@ def main() -> None:
         print(json.dumps(line), flush=True)
 
 
+SERVING_CLASSES = ("exhaustive", "grid", "monte_carlo")
+
+
 def serving_mix(dd, count=48, seed=20261203):
     """Seeded query mix: A uniform over odd 8..16-bit values, k uniform in
     {8,12,16,20,24,32}; k<=20 exhaustive; k>=24 either the grid with stride
-    2^(k-16) or Monte Carlo with 2^32..2^36 Philox samples.  The k=32 grid
-    (2^48 pairs, about a minute of device time for one query) is left out of
-    this timed sample and replaced by its Monte Carlo alternative."""
+    2^(k-16) (m = 2^16 lattice points, so 2^k * 2^16 pairs: 2^48 at k=32) or
+    Monte Carlo with 2^32..2^36 Philox-drawn pairs.  Returns (class, request)."""
     import random
     rng = random.Random(seed)
     out = []
@@ -327,26 +374,35 @@ def serving_mix(dd, count=48, seed=20261203):
         A = rng.randrange(129, 1 << 16) | 1
         k = rng.choice([8, 12, 16, 20, 24, 32])
         if k <= 20:
-            q = dd.Request(dd.CODE_AN, dd.MODE_EXHAUSTIVE, A, k)
-        elif k == 24 and rng.random() < 0.5:
-            q = dd.Request(dd.CODE_AN, dd.MODE_GRID_1D, A, k, m=1 << 16)  # stride 2^(k-16) = 256
+            cls, q = "exhaustive", dd.Request(dd.CODE_AN, dd.MODE_EXHAUSTIVE, A, k)
+        elif rng.random() < 0.5:
+            cls, q = "grid", dd.Request(dd.CODE_AN, dd.MODE_GRID_1D, A, k, m=1 << 16)  # stride 2^(k-16)
         else:
             samples = 1 << rng.randrange(32, 37)
-            q = dd.Request(dd.CODE_AN, dd.MODE_MONTE_CARLO, A, k, m=max(1, samples >> k), seed=i + 1)
+            cls, q = "monte_carlo", dd.Request(dd.CODE_AN, dd.MODE_MONTE_CARLO, A, k, m=max(1, samples >> k),
+                                               seed=i + 1)
         q.user_tag = i
-        out.append(q)
+        out.append((cls, q))
     return out
 
 
+def percentile(sorted_values: list[float], p: float) -> float:
+    """Nearest-rank percentile of an ascending list."""
+    n = len(sorted_values)
+    return sorted_values[min(n - 1, max(0, -(-round(p * 1000) * n // 1000) - 1))]
+
+
 def serving_extra(dd, rate_per_s=16.0) -> dict:
-    """p50/p99 latency (submit -> result) and aggregate pairs/s of the query
-    server on a seeded Poisson stream of the serving mix."""
+    """p50/p99 latency (submit -> result on the host clock), aggregate and per
+    query class, and aggregate pairs/s of the query server on a seeded Poisson
+    stream of the serving mix."""
     import random
     import threading
-    reqs = serving_mix(dd)
+    mix = serving_mix(dd)
+    reqs = [q for _, q in mix]
     rng = random.Random(7)
     with dd.Server(0, round_ms=20) as s:
-        # warm the server (kernel images, autotune-free path)
+        # warm the server (kernel images; the server autotuned when it was created)
         s.wait(s.submit(dd.Request(dd.CODE_AN, dd.MODE_EXHAUSTIVE, 641, 12)), 60)
         tickets = []
         t0 = time.perf_counter()
@@ -359,21 +415,29 @@ def serving_extra(dd, rate_per_s=16.0) -> dict:
         th = threading.Thread(target=client)
         th.start()
         th.join()
-        results = [s.wait(t, 600) for t in tickets]
+        results = [s.wait(t, 900) for t in tickets]
         wall = time.perf_counter() - t0
         st = s.stats()
     assert all(code == 0 for code, _ in results)
     lat = sorted(r.total_ms for _, r in results)
     pairs = sum(r.pairs for _, r in results)
-
-    def pct(p):
-        return lat[min(len(lat) - 1, max(0, int(-(-p * len(lat) // 1)) - 1))]
-
-    return {"queries": len(reqs), "arrival_rate_per_s": rate_per_s, "p50_ms": pct(0.50), "p99_ms": pct(0.99),
+    per_class = {}
+    for cls in SERVING_CLASSES:
+        rows = [(q, r) for (c, q), (_, r) in zip(mix, results) if c == cls]
+        if not rows:
+            continue
+        cl = sorted(r.total_ms for _, r in rows)
+        per_class[cls] = {"queries": len(rows), "p50_ms": percentile(cl, 0.50), "p99_ms": percentile(cl, 0.99),
+                          "max_ms": cl[-1], "pairs": sum(r.pairs for _, r in rows),
+                          "k": sorted({q.n for q, _ in rows})}
+    kernels = {r.kernel_used for _, r in results}
+    return {"queries": len(reqs), "arrival_rate_per_s": rate_per_s, "p50_ms": percentile(lat, 0.50),
+            "p99_ms": percentile(lat, 0.99), "per_class": per_class,
             "pairs": pairs, "pairs_per_s_wall": pairs / wall, "pairs_per_s_device": st["pairs_per_s"],
             "rounds": st["rounds"], "wall_s": wall,
+            "kernels_used": sorted({dd.KERNEL_POPC: "popc", dd.KERNEL_MMA: "mma"}.get(x, str(x)) for x in kernels),
             "mix": "A odd 8-16 bit, k in {8,12,16,20,24,32}; exhaustive k<=20; k>=24 grid stride 2^(k-16) "
-                   "(k=24) or MC 2^32..2^36 samples; k=32 grid left out of the timed sample"}
+                   "(m=2^16) or Monte Carlo 2^32..2^36 samples"}
 
 
 def super_a_set(count=256, seed=20261203):
@@ -388,13 +452,20 @@ def super_a_set(count=256, seed=20261203):
 
 
 def super_a_extra(ctx, dd) -> dict:
-    """k=16 sweep over 256 seeded odd A in [32768, 65536): ONE persistent,
-    graph-captured launch for all instances vs the plain baseline (one launch
-    per instance, bins allocated/copied/freed per call, dd_histogram_plain)."""
+    """k=16 sweep over 256 seeded odd A in [32768, 65536), three ways:
+      batched_*   ONE persistent, graph-captured launch for all 256 instances;
+      single_*    256 dd_histogram calls, one persistent launch per instance
+                  (the reference's loop over A, super_a/src/main.cpp:247-297,
+                  on this GPU's kernels);
+      plain       256 dd_histogram_plain calls (the reference's kernel design:
+                  one thread per row, bins allocated/copied/freed per call).
+    speedup_vs_single_launch isolates batching + graph replay; speedup_vs_plain
+    adds the kernel design."""
     As = super_a_set()
     reqs = [dd.Request(dd.CODE_AN, dd.MODE_EXHAUSTIVE, A, 16, convention=dd.CONV_SUPER_A) for A in As]
     P = pairs_of(16) * len(As)
     out = {}
+    batched = None
     for name, kernel in (("batched_popc", dd.KERNEL_POPC), ("batched_mma", dd.KERNEL_MMA)):
         for _ in range(3):
             ctx.batch(reqs, use_graph=True, kernel=kernel)
@@ -405,8 +476,23 @@ def super_a_extra(ctx, dd) -> dict:
         wall = (time.perf_counter() - t) / reps
         out[name] = {"pairs_per_s": P / wall, "kernel_pairs_per_s": P / (res[0].kernel_ms * 1e-3),
                      "wall_s": wall}
-        out.setdefault("_results", res)
-    batched = out.pop("_results")
+        batched = batched or res
+    singles = {}
+    for name, kernel in (("single_popc", dd.KERNEL_POPC), ("single_mma", dd.KERNEL_MMA)):
+        one = [dd.Request(dd.CODE_AN, dd.MODE_EXHAUSTIVE, A, 16, convention=dd.CONV_SUPER_A, kernel=kernel)
+               for A in As]
+        for q in one[:8]:
+            ctx.histogram(q)
+        t = time.perf_counter()
+        kernel_s = 0.0
+        got = []
+        for q in one:
+            r = ctx.histogram(q)
+            kernel_s += r.kernel_ms * 1e-3
+            got.append(r)
+        wall = time.perf_counter() - t
+        assert all(a.counts == b.counts for a, b in zip(batched, got)), f"batched != {name}"
+        singles[name] = {"pairs_per_s": P / wall, "kernel_pairs_per_s": P / kernel_s, "wall_s": wall}
     for r in reqs[:8]:
         ctx.histogram_plain(r)
     t = time.perf_counter()
@@ -419,10 +505,13 @@ def super_a_extra(ctx, dd) -> dict:
     plain_wall = time.perf_counter() - t
     assert all(a.counts == b.counts for a, b in zip(batched, plain)), "batched != plain"
     best = max(out.values(), key=lambda v: v["pairs_per_s"])
+    best_single = max(singles.values(), key=lambda v: v["pairs_per_s"])
+    out.update(singles)
     out.update({"instances": len(As), "k": 16, "pairs": P,
                 "plain_pairs_per_s": P / plain_wall, "plain_kernel_pairs_per_s": P / plain_kernel,
                 "plain_wall_s": plain_wall,
-                "speedup_vs_plain": plain_wall / best["wall_s"]})
+                "speedup_vs_plain": plain_wall / best["wall_s"],
+                "speedup_vs_single_launch": best_single["wall_s"] / best["wall_s"]})
     return out
 
 

@@ -22,7 +22,8 @@ from pathlib import Path
 __all__ = [
     "CODE_AN", "CODE_EXT_HAMMING", "MODE_EXHAUSTIVE", "MODE_GRID_1D", "MODE_GRID_2D", "MODE_MONTE_CARLO",
     "KERNEL_AUTO", "KERNEL_POPC", "KERNEL_MMA", "HAMMING_WEIGHTS", "HAMMING_ALL_PAIRS", "HAMMING_ALL_PAIRS_DISTINCT",
-    "CONV_GPU", "CONV_CPU", "CONV_SUPER_A", "MAX_BINS", "DDError", "Request", "Result", "Context", "Server",
+    "CONV_GPU", "CONV_CPU", "CONV_SUPER_A", "MMA_EPILOGUE_AUTO", "MMA_EPILOGUE_PAIRED",
+    "MMA_EPILOGUE_SINGLE", "MAX_BINS", "DDError", "Request", "Result", "Context", "Server",
     "load", "lib_path", "postprocess", "request_plan", "format_result", "request_shape", "philox4x32_10", "device_count",
     "run_ancoding", "run_ancoding_cpu", "run_ancoding_grid", "run_ancoding_mc", "run_hamming",
     "run_hamming_grid", "run_hamming_mc",
@@ -33,6 +34,8 @@ MODE_EXHAUSTIVE, MODE_GRID_1D, MODE_GRID_2D, MODE_MONTE_CARLO = 0, 1, 2, 3
 KERNEL_AUTO, KERNEL_POPC, KERNEL_MMA = 0, 1, 2
 HAMMING_WEIGHTS, HAMMING_ALL_PAIRS, HAMMING_ALL_PAIRS_DISTINCT = 0, 1, 2
 CONV_GPU, CONV_CPU, CONV_SUPER_A = 0, 1, 2
+MMA_EPILOGUE_AUTO, MMA_EPILOGUE_PAIRED, MMA_EPILOGUE_SINGLE = 0, 1, 2
+EPILOGUE_NAMES = {0: "none", 1: "paired", 2: "single"}
 MAX_BINS = 64
 
 STATUS = {
@@ -67,13 +70,19 @@ class _Res(C.Structure):
                 ("raw", C.c_uint64 * MAX_BINS), ("counts_lo", C.c_uint64 * MAX_BINS),
                 ("counts_hi", C.c_uint64 * MAX_BINS), ("minb", C.c_uint64), ("mincb_lo", C.c_uint64),
                 ("mincb_hi", C.c_uint64), ("max_rel_error", C.c_double), ("kernel_ms", C.c_double),
-                ("total_ms", C.c_double), ("user_tag", C.c_uint64)]
+                ("total_ms", C.c_double), ("user_tag", C.c_uint64), ("mma_epilogue", C.c_uint32),
+                ("reserved", C.c_uint32)]
 
 
 class _Tuning(C.Structure):
     _fields_ = [("kernel", C.c_uint32), ("hist_mode", C.c_uint32), ("popc_red_pairs_per_s", C.c_double),
                 ("popc_ldst_pairs_per_s", C.c_double), ("mma_pairs_per_s", C.c_double),
-                ("probe_pairs", C.c_uint64)]
+                ("probe_pairs", C.c_uint64), ("mma_paired_pairs_per_s", C.c_double),
+                ("mma_epilogue", C.c_uint32), ("reserved", C.c_uint32)]
+
+
+class _RedProbe(C.Structure):
+    _fields_ = [("warps_per_sm", C.c_uint32), ("pattern", C.c_uint32), ("adds_per_s", C.c_double)]
 
 
 class _CandRes(C.Structure):
@@ -126,6 +135,7 @@ class Result:
     iterations2: int
     kernel_used: int
     user_tag: int = 0
+    mma_epilogue: int = 0
     _c: object = field(default=None, repr=False)
 
     @staticmethod
@@ -137,7 +147,7 @@ class Result:
             minb=r.minb, mincb=(r.mincb_hi << 64) | r.mincb_lo, max_rel_error=r.max_rel_error,
             kernel_ms=r.kernel_ms, total_ms=r.total_ms, pairs=(r.pairs_hi << 64) | r.pairs_lo,
             iterations=r.iterations, iterations2=r.iterations2, kernel_used=r.kernel_used,
-            user_tag=r.user_tag, _c=r)
+            user_tag=r.user_tag, mma_epilogue=r.mma_epilogue, _c=r)
 
 
 _lib = None
@@ -174,7 +184,9 @@ def load() -> C.CDLL:
     lib.dd_philox4x32_10.restype = None
     lib.dd_measure_popc_peak.argtypes = [vp, C.POINTER(C.c_double)]
     lib.dd_measure_red_peak.argtypes = [vp, C.POINTER(C.c_double)]
+    lib.dd_measure_red_sweep.argtypes = [vp, vp, u32, C.POINTER(C.c_uint32)]
     lib.dd_set_wait_timeout.argtypes = [vp, C.c_uint64]
+    lib.dd_set_mma_epilogue.argtypes = [vp, u32]
     lib.dd_autotune.argtypes = [vp, C.POINTER(_Tuning)]
     lib.dd_mc_extend.argtypes = [vp, C.POINTER(_Req), C.c_uint64, C.POINTER(C.c_uint64), C.POINTER(_Res)]
     lib.dd_an_candidates.argtypes = [vp, u32, u32, C.POINTER(C.c_uint64), C.c_uint64, C.POINTER(_CandRes)]
@@ -350,8 +362,15 @@ class Context:
         _check(load().dd_autotune(self._h, C.byref(t)))
         return {"kernel": "mma" if t.kernel == KERNEL_MMA else "popc",
                 "hist_mode": "red" if t.hist_mode == 0 else "ldst",
+                "mma_epilogue": EPILOGUE_NAMES.get(t.mma_epilogue, str(t.mma_epilogue)),
                 "popc_red_pairs_per_s": t.popc_red_pairs_per_s, "popc_ldst_pairs_per_s": t.popc_ldst_pairs_per_s,
-                "mma_pairs_per_s": t.mma_pairs_per_s, "probe_pairs": t.probe_pairs}
+                "mma_single_pairs_per_s": t.mma_pairs_per_s, "mma_paired_pairs_per_s": t.mma_paired_pairs_per_s,
+                "probe_pairs": t.probe_pairs}
+
+    def set_mma_epilogue(self, epilogue: int) -> None:
+        """Epilogue of this context's tcgen05 launches: MMA_EPILOGUE_AUTO (the
+        autotuner's choice), MMA_EPILOGUE_PAIRED or MMA_EPILOGUE_SINGLE."""
+        _check(load().dd_set_mma_epilogue(self._h, epilogue))
 
     def popc_peak(self) -> float:
         v = C.c_double()
@@ -363,10 +382,22 @@ class Context:
         _check(load().dd_set_wait_timeout(self._h, ns))
 
     def red_peak(self) -> float:
-        """Shared-memory atomic adds per second (the tcgen05 epilogue's bound)."""
+        """Shared-memory atomic adds per second (the tcgen05 epilogue's bound):
+        the maximum of red_sweep()."""
         v = C.c_double()
         _check(load().dd_measure_red_peak(self._h, C.byref(v)))
         return v.value
+
+    def red_sweep(self) -> list[dict]:
+        """The shared-memory atomic rate at 8..32 warps per SM for the per-thread
+        column pattern (single epilogue) and the shared lane-column pattern
+        (paired epilogue)."""
+        rows = (_RedProbe * 64)()
+        n = C.c_uint32()
+        _check(load().dd_measure_red_sweep(self._h, rows, 64, C.byref(n)))
+        return [{"warps_per_sm": rows[i].warps_per_sm,
+                 "pattern": "per_thread_columns" if rows[i].pattern == 0 else "lane_columns_shared",
+                 "adds_per_s": rows[i].adds_per_s} for i in range(n.value)]
 
     def an_candidates(self, k: int, a_bits: int, capacity: int | None = None) -> tuple[dict, list[int]]:
         """dd_an_candidates: the super-A candidates of (k data bits, A width

@@ -41,6 +41,8 @@ struct dd_context {
   // tuning
   int hist_mode = dd::HIST_RED;
   int tuned = 0;
+  uint32_t mma_epilogue = DD_MMA_EPILOGUE_AUTO;         // requested (dd_set_mma_epilogue)
+  uint32_t mma_tuned_epilogue = DD_MMA_EPILOGUE_PAIRED;  // the autotuner's verdict for AUTO
   unsigned long long mma_timeout_ns = 2000000000ull;  // bound of every device-side wait
   // batch graph cache
   cudaGraphExec_t gexec = nullptr;
@@ -106,6 +108,11 @@ struct LaunchPlan {
   uint32_t nmma = 0;
   uint32_t nslots = 0;       // bin slots (one per request, in request order)
 };
+
+// Epilogue of the context's tcgen05 launches.
+static uint32_t mma_epilogue_of(const dd_context* ctx) {
+  return ctx->mma_epilogue == DD_MMA_EPILOGUE_AUTO ? ctx->mma_tuned_epilogue : ctx->mma_epilogue;
+}
 
 // Which kernel runs a job: explicit MMA or POPC requests are honoured where
 // the job allows them; AUTO uses the context's measured preference.
@@ -177,9 +184,22 @@ static int plan_launch(dd_context* ctx, std::vector<Job>& jobs, const std::vecto
   lp.margs.counter = ctx->d_ctl + 1;
   lp.margs.status = status;
   lp.margs.timeout_ns = ctx->mma_timeout_ns;
+  lp.margs.packed = mma_epilogue_of(ctx) == DD_MMA_EPILOGUE_PAIRED ? 1u : 0u;
+  lp.margs.pk_cells = 0;
+  lp.margs.pad = 0;
   if (lp.nmma && tm) {
-    lp.margs.b_bufs = mma_b_bufs(lp.margs.hist_rows);
-    lp.msmem = mma_smem_bytes(lp.margs.hist_rows, lp.margs.b_bufs);
+    if (lp.margs.packed) {
+      // one joint table for the launch, sized for its largest S; each job's
+      // window of d2 rows and its packing parameters follow from it
+      uint32_t smax = 1;
+      for (uint32_t k = lp.npopc; k < table.size(); ++k)
+        smax = std::max(smax, (uint32_t)mma_max_distance(table[k]) + 1u);
+      mma_pk_layout(smax, &lp.margs.pk_cells, &lp.margs.b_bufs);
+      for (uint32_t k = lp.npopc; k < table.size(); ++k) mma_pack_setup(table[k], lp.margs.pk_cells);
+    } else {
+      lp.margs.b_bufs = mma_b_bufs(lp.margs.hist_rows);
+    }
+    lp.msmem = mma_smem_bytes(lp.margs.hist_rows, lp.margs.b_bufs, lp.margs.packed != 0, lp.margs.pk_cells);
     lp.mgrid = (int)std::min<uint64_t>((uint64_t)ctx->num_sms, tm);  // one CTA (one TMEM owner) per SM
   }
   std::memcpy(ctx->h_jobs, table.data(), table.size() * sizeof(Job));
@@ -250,6 +270,7 @@ int launch_round(dd_context* ctx, std::vector<Job>& jobs, const std::vector<uint
 }
 
 bool uses_mma(const dd_context* ctx, const Job& j, uint32_t kernel) { return want_mma(ctx, j, kernel); }
+uint32_t mma_epilogue_used(const dd_context* ctx) { return mma_epilogue_of(ctx); }
 void* context_stream(const dd_context* ctx) { return (void*)ctx->stream; }
 int context_device(const dd_context* ctx) { return ctx->device; }
 
@@ -493,6 +514,7 @@ static int run_requests(dd_context* ctx, const dd_request* reqs, uint32_t count,
     postprocess(reqs[i], shapes[i], raw, r);
     fill_pairs(r, pairs);
     r.kernel_used = want_mma(ctx, jobs[i], kernels[i]) ? DD_KERNEL_MMA : DD_KERNEL_POPC;
+    r.mma_epilogue = r.kernel_used == DD_KERNEL_MMA ? mma_epilogue_of(ctx) : 0u;
     r.kernel_ms = ms;  // one launch: the whole batch's device time
     r.total_ms = total;
     r.user_tag = reqs[i].user_tag;
@@ -514,10 +536,12 @@ int dd_autotune(dd_context* ctx, dd_tuning* out) {
   q.A = 65521;
   q.n = 20;  // large enough that every kernel reaches its steady state (0.1 s per run)
   const uint64_t pairs = (1ull << 20) * ((1ull << 20) - 1) / 2;
-  auto best_ms = [&](uint32_t kernel, int mode, double* ms_out) -> int {
+  auto best_ms = [&](uint32_t kernel, int mode, uint32_t epilogue, double* ms_out) -> int {
     const int saved_mode = ctx->hist_mode, saved_tuned = ctx->tuned;
+    const uint32_t saved_epi = ctx->mma_epilogue;
     ctx->hist_mode = mode;
     ctx->tuned = 1;  // keep AUTO out of the way while probing
+    ctx->mma_epilogue = epilogue;
     q.kernel = kernel;
     double best = 1e30;
     int st = DD_OK;
@@ -528,22 +552,28 @@ int dd_autotune(dd_context* ctx, dd_tuning* out) {
     }
     ctx->hist_mode = saved_mode;
     ctx->tuned = saved_tuned;
+    ctx->mma_epilogue = saved_epi;
     *ms_out = best;
     return st;
   };
-  double red = 0, ldst = 0, mma = 0;
-  int st = best_ms(DD_KERNEL_POPC, HIST_RED, &red);
-  if (st == DD_OK) st = best_ms(DD_KERNEL_POPC, HIST_LDST, &ldst);
-  if (st == DD_OK) st = best_ms(DD_KERNEL_MMA, ctx->hist_mode, &mma);
+  double red = 0, ldst = 0, mma = 0, paired = 0;
+  int st = best_ms(DD_KERNEL_POPC, HIST_RED, DD_MMA_EPILOGUE_AUTO, &red);
+  if (st == DD_OK) st = best_ms(DD_KERNEL_POPC, HIST_LDST, DD_MMA_EPILOGUE_AUTO, &ldst);
+  if (st == DD_OK) st = best_ms(DD_KERNEL_MMA, ctx->hist_mode, DD_MMA_EPILOGUE_SINGLE, &mma);
+  if (st == DD_OK) st = best_ms(DD_KERNEL_MMA, ctx->hist_mode, DD_MMA_EPILOGUE_PAIRED, &paired);
   if (st != DD_OK) return st;
   ctx->hist_mode = red <= ldst ? HIST_RED : HIST_LDST;
-  ctx->tuned = mma < std::min(red, ldst) ? 2 : 1;
+  ctx->mma_tuned_epilogue = paired <= mma ? DD_MMA_EPILOGUE_PAIRED : DD_MMA_EPILOGUE_SINGLE;
+  ctx->tuned = std::min(mma, paired) < std::min(red, ldst) ? 2 : 1;
   if (out) {
+    std::memset(out, 0, sizeof(*out));
     out->kernel = ctx->tuned == 2 ? DD_KERNEL_MMA : DD_KERNEL_POPC;
     out->hist_mode = (uint32_t)ctx->hist_mode;
     out->popc_red_pairs_per_s = pairs / (red * 1e-3);
     out->popc_ldst_pairs_per_s = pairs / (ldst * 1e-3);
     out->mma_pairs_per_s = pairs / (mma * 1e-3);
+    out->mma_paired_pairs_per_s = pairs / (paired * 1e-3);
+    out->mma_epilogue = ctx->mma_tuned_epilogue;
     out->probe_pairs = pairs;
   }
   return DD_OK;
@@ -707,33 +737,63 @@ int dd_measure_popc_peak(dd_context* ctx, double* popc_per_s) {
   return DD_OK;
 }
 
+int dd_set_mma_epilogue(dd_context* ctx, uint32_t epilogue) {
+  if (!ctx) { set_error("NULL argument"); return DD_ERR_INVALID_ARGUMENT; }
+  if (epilogue > DD_MMA_EPILOGUE_SINGLE) { set_error("unknown tcgen05 epilogue"); return DD_ERR_INVALID_ARGUMENT; }
+  ctx->mma_epilogue = epilogue;
+  return DD_OK;
+}
+
 int dd_set_wait_timeout(dd_context* ctx, uint64_t ns) {
   if (!ctx) { set_error("NULL argument"); return DD_ERR_INVALID_ARGUMENT; }
   ctx->mma_timeout_ns = ns ? ns : 2000000000ull;
   return DD_OK;
 }
 
-int dd_measure_red_peak(dd_context* ctx, double* adds_per_s) {
-  if (!ctx || !adds_per_s) { set_error("NULL argument"); return DD_ERR_INVALID_ARGUMENT; }
+int dd_measure_red_sweep(dd_context* ctx, dd_red_probe* out, uint32_t cap, uint32_t* count) {
+  if (!ctx || !out || !count) { set_error("NULL argument"); return DD_ERR_INVALID_ARGUMENT; }
+  *count = 0;
   DD_CUDA(cudaSetDevice(ctx->device));
   uint32_t* sink = nullptr;
   const int grid = ctx->num_sms;
   DD_CUDA(cudaMalloc(&sink, grid * sizeof(uint32_t)));
   const uint32_t iters = 20000;
-  cudaError_t e = launch_red_rate(iters / 10, grid, sink, ctx->stream);  // warm-up
-  float best = 1e30f;
-  for (int rep = 0; rep < 3 && e == cudaSuccess; ++rep) {
-    e = cudaEventRecord(ctx->ev0, ctx->stream);
-    if (e == cudaSuccess) e = launch_red_rate(iters, grid, sink, ctx->stream);
-    if (e == cudaSuccess) e = cudaEventRecord(ctx->ev1, ctx->stream);
-    if (e == cudaSuccess) e = cudaEventSynchronize(ctx->ev1);
-    float ms = 0;
-    if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
-    if (e == cudaSuccess && ms < best) best = ms;
-  }
+  cudaError_t e = cudaSuccess;
+  for (int pattern = 0; pattern < 2 && e == cudaSuccess; ++pattern)
+    for (int warps = 8; warps <= 32 && e == cudaSuccess; warps += 4) {
+      const int threads = warps * 32;
+      e = launch_red_rate(iters / 10, grid, threads, pattern, sink, ctx->stream);  // warm-up
+      float best = 1e30f;
+      for (int rep = 0; rep < 3 && e == cudaSuccess; ++rep) {
+        e = cudaEventRecord(ctx->ev0, ctx->stream);
+        if (e == cudaSuccess) e = launch_red_rate(iters, grid, threads, pattern, sink, ctx->stream);
+        if (e == cudaSuccess) e = cudaEventRecord(ctx->ev1, ctx->stream);
+        if (e == cudaSuccess) e = cudaEventSynchronize(ctx->ev1);
+        float ms = 0;
+        if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+        if (e == cudaSuccess && ms < best) best = ms;
+      }
+      if (e == cudaSuccess && *count < cap) {
+        dd_red_probe& r = out[(*count)++];
+        r.warps_per_sm = (uint32_t)warps;
+        r.pattern = (uint32_t)pattern;
+        r.adds_per_s = (double)red_rate_adds(iters, grid, threads) / (best * 1e-3);
+      }
+    }
   cudaFree(sink);
   if (e != cudaSuccess) return cuda_fail(e, "shared-atomic probe");
-  *adds_per_s = (double)red_rate_adds(iters, grid) / (best * 1e-3);
+  return DD_OK;
+}
+
+int dd_measure_red_peak(dd_context* ctx, double* adds_per_s) {
+  if (!ctx || !adds_per_s) { set_error("NULL argument"); return DD_ERR_INVALID_ARGUMENT; }
+  dd_red_probe rows[64];
+  uint32_t n = 0;
+  const int st = dd_measure_red_sweep(ctx, rows, 64, &n);
+  if (st != DD_OK) return st;
+  double best = 0;
+  for (uint32_t i = 0; i < n; ++i) best = std::max(best, rows[i].adds_per_s);
+  *adds_per_s = best;
   return DD_OK;
 }
 

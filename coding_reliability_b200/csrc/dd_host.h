@@ -63,6 +63,7 @@ void set_error(const std::string& msg);
 // accumulated across rounds (the bins are not reset).
 int launch_round(dd_context* ctx, std::vector<Job>& jobs, const std::vector<uint32_t>& kernels, float* kernel_ms);
 bool uses_mma(const dd_context* ctx, const Job& j, uint32_t kernel);
+uint32_t mma_epilogue_used(const dd_context* ctx);  // dd_mma_epilogue of the context's tcgen05 launches
 void* context_stream(const dd_context* ctx);
 int context_device(const dd_context* ctx);
 

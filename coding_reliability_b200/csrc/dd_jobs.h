@@ -74,10 +74,13 @@ struct Job {
   uint32_t wgen;             // WeightGen
   uint32_t bucket;           // Ext-Hamming template bucket N (8 for n in {4,8})
   uint32_t shard;            // Ext-Hamming grid: Shards<N>
-  uint32_t pad;
+  uint32_t pk_s;             // tcgen05 pair-packed epilogue: S = largest distance + 1, the packed
+                             // value of a distance pair (d1, d2) is d1 + S * (d2 - pk_lo)
   uint64_t tile_offset;      // first tile of the instance this job covers (a launch may run a
                              // sub-range [tile_offset, tile_offset + tiles) of the instance)
   uint64_t sample_begin;     // MC: every codeword draws its samples [sample_begin, iters) only
+  int32_t pk_lo;             // tcgen05 pair-packed epilogue: first d2 of the joint-bin window
+  uint32_t pk_limit;         // tcgen05 pair-packed epilogue: packed values below it are table cells
 };
 
 // Status bits a kernel reports back (the word is zeroed before each launch).

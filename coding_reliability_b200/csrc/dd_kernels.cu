@@ -554,29 +554,44 @@ __global__ void __launch_bounds__(256) popc_rate_kernel(uint32_t iters, uint32_t
   if (r == 0x12345678u) sink[blockIdx.x] = r;
 }
 
-// Shared-memory atomic issue rate, as the tcgen05 kernel's epilogue uses it:
-// one CTA of 512 threads per SM, each thread adds 1 to its own column of a
-// 32-row x 512-column table (row stride 2 KB, so a warp's 32 lanes hit 32
-// banks), the row changing with every add.
-constexpr int kRedThreads = 512;
+// Shared-memory atomic rate, measured the way the tcgen05 kernel's epilogues
+// use the pipe: one CTA per SM of blockDim.x threads, every thread adding 1 in
+// a 128 KB table, 32 independent adds per loop iteration, conflict-free within
+// each warp (the 32 lanes always hit 32 banks).
+//   kRedPerThread: every thread its own column of 32 rows (row stride
+//                  blockDim.x words), the row changing with every add (the
+//                  single epilogue's per-thread bins);
+//   kRedLaneShared: one column per lane shared by every warp of the CTA, 1024
+//                  cells, the cell changing with every add and differing
+//                  between warps (the paired epilogue's joint table).
 constexpr int kRedRows = 32;
+constexpr uint32_t kRedCells = 1024;
+enum RedPattern : int { kRedPerThread = 0, kRedLaneShared = 1 };
 
-__global__ void __launch_bounds__(kRedThreads, 1) red_rate_kernel(uint32_t iters, uint32_t* sink) {
-  extern __shared__ uint32_t tab[];  // kRedRows x kRedThreads
-  for (int k = threadIdx.x; k < kRedRows * kRedThreads; k += kRedThreads) tab[k] = 0;
+template <int kPattern>
+__global__ void __launch_bounds__(1024, 1) red_rate_kernel(uint32_t iters, uint32_t* sink) {
+  extern __shared__ uint32_t tab[];
+  const uint32_t nthr = blockDim.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const uint32_t words = kPattern == kRedPerThread ? kRedRows * nthr : kRedCells * 32u;
+  for (uint32_t k = tid; k < words; k += nthr) tab[k] = 0;
   __syncthreads();
-  const uint32_t base = (uint32_t)__cvta_generic_to_shared(tab) + threadIdx.x * 4u;
+  const uint32_t sbase = (uint32_t)__cvta_generic_to_shared(tab);
   for (uint32_t i = 0; i < iters; ++i) {
 #pragma unroll
-    for (int u = 0; u < 32; ++u) {
-      const uint32_t row = (i + (uint32_t)u * 7u) & (kRedRows - 1);
-      asm volatile("red.shared.add.u32 [%0], 1;" ::"r"(base + (row << 11)) : "memory");
+    for (uint32_t u = 0; u < 32; ++u) {
+      uint32_t a;
+      if constexpr (kPattern == kRedPerThread) {
+        a = sbase + tid * 4u + (((i + u * 7u) & (kRedRows - 1)) * nthr) * 4u;
+      } else {
+        a = sbase + lane * 4u + (((i * 32u + u) * 37u + warp * 101u) & (kRedCells - 1)) * 128u;
+      }
+      asm volatile("red.shared.add.u32 [%0], 1;" ::"r"(a) : "memory");
     }
   }
   __syncthreads();
   uint32_t s = 0;
-  for (int r = 0; r < kRedRows; ++r) s += tab[r * kRedThreads + threadIdx.x];
-  if (s != iters * 32u) sink[blockIdx.x] = s;  // never for a correct run; keeps the adds alive
+  for (uint32_t k = tid; k < words; k += nthr) s += tab[k];
+  if (s == 0x9E3779B9u) sink[blockIdx.x] = s;  // keeps the adds alive (the value is irrelevant)
 }
 
 // ---------------------------------------------------------------------------
@@ -590,14 +605,24 @@ static const void* kernel_ptr(int mode) {
   return mode == HIST_RED ? (const void*)hist_kernel<HIST_RED> : (const void*)hist_kernel<HIST_LDST>;
 }
 
+// The dynamic shared-memory limit of hist_kernel is a per-function attribute
+// shared by every host thread, so every caller sets the same value: the largest
+// any plan asks for (kMaxBins bin rows and the column table).  A per-launch
+// value could be lowered by one thread between another's set and launch.
+static cudaError_t hist_smem_limit(int mode, size_t smem) {
+  const size_t limit = hist_smem_bytes(kMaxBins, true);
+  if (smem > limit) return cudaErrorInvalidValue;
+  return cudaFuncSetAttribute(kernel_ptr(mode), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)limit);
+}
+
 cudaError_t hist_occupancy(int mode, size_t smem, int* ctas_per_sm) {
-  cudaError_t e = cudaFuncSetAttribute(kernel_ptr(mode), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaError_t e = hist_smem_limit(mode, smem);
   if (e != cudaSuccess) return e;
   return cudaOccupancyMaxActiveBlocksPerMultiprocessor(ctas_per_sm, kernel_ptr(mode), kWarpsPerCta * 32, smem);
 }
 
 cudaError_t launch_hist(int mode, const LaunchArgs& args, int grid, size_t smem, cudaStream_t stream) {
-  cudaError_t e = cudaFuncSetAttribute(kernel_ptr(mode), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaError_t e = hist_smem_limit(mode, smem);
   if (e != cudaSuccess) return e;
   if (mode == HIST_RED)
     hist_kernel<HIST_RED><<<grid, kWarpsPerCta * 32, smem, stream>>>(args);
@@ -611,14 +636,20 @@ cudaError_t launch_popc_rate(uint32_t iters, int grid, uint32_t* sink, cudaStrea
   return cudaGetLastError();
 }
 
-// One CTA per SM: the table needs 64 KB, the launch asks for more than half an SM.
-cudaError_t launch_red_rate(uint32_t iters, int grid, uint32_t* sink, cudaStream_t stream) {
-  const int smem = 120 * 1024;
-  cudaError_t e = cudaFuncSetAttribute(red_rate_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+// One CTA per SM: the tables need 128 KB, the launch asks for more than half an SM.
+cudaError_t launch_red_rate(uint32_t iters, int grid, int threads, int pattern, uint32_t* sink, cudaStream_t stream) {
+  const int smem = 132 * 1024;
+  if (threads < 32 || threads > 1024 || threads % 32) return cudaErrorInvalidValue;
+  const void* fn = pattern == kRedLaneShared ? (const void*)red_rate_kernel<kRedLaneShared>
+                                             : (const void*)red_rate_kernel<kRedPerThread>;
+  cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   if (e != cudaSuccess) return e;
-  red_rate_kernel<<<grid, kRedThreads, smem, stream>>>(iters, sink);
+  if (pattern == kRedLaneShared)
+    red_rate_kernel<kRedLaneShared><<<grid, threads, smem, stream>>>(iters, sink);
+  else
+    red_rate_kernel<kRedPerThread><<<grid, threads, smem, stream>>>(iters, sink);
   return cudaGetLastError();
 }
-uint64_t red_rate_adds(uint32_t iters, int grid) { return (uint64_t)grid * kRedThreads * iters * 32u; }
+uint64_t red_rate_adds(uint32_t iters, int grid, int threads) { return (uint64_t)grid * threads * iters * 32u; }
 
 }  // namespace dd

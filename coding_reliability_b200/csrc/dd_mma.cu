@@ -3,38 +3,58 @@
 //
 // The Hamming distance of two codewords x, y (bit planes b_x, b_y in {0,1}^L)
 // is d = popc(x) + popc(y) - 2<b_x, b_y>.  The operands put that whole
-// expression into one int8 GEMM with K = 64:
+// expression into one int8 GEMM with K = 64.  Two epilogue variants:
+//
+// Single (one distance per MMA column):
 //   A row i    (codeword x_i): bytes k<L: -2*b_ik;  byte L: popc(x_i);  byte L+1: 1
 //   B column j (codeword y_j): bytes k<L:    b_jk;  byte L: 1;          byte L+1: popc(y_j)
-// so the INT32 accumulator D[i][j] = Σ_k A[i][k]·B[k][j] is exactly d(i, j).
-// The epilogue reads D from TMEM (tcgen05.ld) and bumps one shared-memory bin
-// per pair; no other per-pair arithmetic is left.
+// so the INT32 accumulator D[i][j] is exactly d(i, j); the epilogue bumps one
+// shared-memory bin per pair (per-thread bin columns).
+//
+// Pair-packed (two distances per MMA column): column p carries two codewords y
+// and y' (columns j and j + 512 of the strip), with S = largest distance + 1:
+//   A row i:    bytes k<L: -2*b_ik;            byte L: popc(x_i); byte L+1: S;              byte L+2: 1
+//   B column p: bytes k<L: b_yk + S*b_y'k;     byte L: 1 + S;     byte L+1: popc(y') - lo;  byte L+2: popc(y)
+// so D[i][p] = d(x_i, y) + S*(d(x_i, y') - lo), every byte within int8.  That
+// value is directly the cell of a joint (d1, d2) table of 1024 cells whenever
+// d2 lies in the window [lo, lo + 1024/S) chosen on the host from the job's
+// distance distribution: one shared-memory atomic counts two pairs.  The OR of
+// a tile's values shows at once whether any lies outside [0, 1024); only then
+// are values checked one by one and the outliers counted as two single
+// distances in a fallback row.  The table has one column per lane, shared by
+// all epilogue warps, and is folded into the job's bins (row sums for d2,
+// column sums for d1) when the job changes, every kPkFlushTiles tiles and at
+// exit, between two bounded epilogue-wide barriers.  It also halves the MMAs,
+// tensor-memory loads and column-operand bytes per pair.
 //
 // Work unit: the popc kernel's tile space (1024x1024 super tiles of the i<j
 // triangle, split into 8 strips of 128 rows; for grid jobs, 128 lattice rows x
 // 1024 columns, taken column-major).  A strip is 128 rows (UMMA M) x
-// 1024 columns = 4 MMA tiles of N = 256, accumulated in two TMEM buffers of 256
-// columns: the MMA of tile t+1 runs while the epilogue bins tile t.  (Four
-// buffers of N = 128 measured 17 % slower: every tile costs each epilogue warp
-// a barrier poll and an arrive through the shared-memory pipe that its atomics
-// saturate, so fewer, wider tiles win over deeper buffering.)  Generator warps
-// claim 8 strips at a time (one super tile when the job's tile range is
-// aligned) and write the column operand once per super tile, into the second
-// of two buffers when both fit beside the bins, so the next super tile's
-// operand is written while the current one's MMAs run; the row operand is
-// double-buffered by strip.
-// One CTA per SM (16 epilogue warps, 1 issuer warp, 3 generator warps, 512 TMEM
-// columns).
+// 1024 columns = 4 MMA tiles of N = 256 (single) or 2 tiles of N = 256 packed
+// columns, accumulated in two TMEM buffers of 256 columns: the MMA of tile t+1
+// runs while the epilogue bins tile t.  (Four buffers of N = 128 measured 17 %
+// slower for the single epilogue: every tile costs each epilogue warp a barrier
+// poll and an arrive through the shared-memory pipe that its atomics saturate,
+// so fewer, wider tiles win over deeper buffering.)  Generator warps claim 8
+// strips at a time (one super tile when the job's tile range is aligned) and
+// write the column operand once per super tile, into the second of two
+// buffers when both fit beside the bins, so the next super tile's operand is
+// written while the current one's MMAs run; the row operand is double-buffered
+// by strip.  One CTA per SM (16 epilogue warps, 1 issuer warp, 3 generator
+// warps, 512 TMEM columns).
 //
-// The epilogue is bound by the shared-memory atomic rate (one red.shared per
-// pair; about 31 per clock per SM measured on B200), twice the POPC issue rate
-// (16 per clock per SM) that bounds the popc kernel.  A waiting epilogue warp
+// The single epilogue is bound by the shared-memory atomic rate (one
+// red.shared per pair; about 31 per clock per SM measured on B200), twice the
+// POPC issue rate (16 per clock per SM) that bounds the popc kernel; the
+// pair-packed epilogue needs one atomic per two pairs.  A waiting epilogue warp
 // pauses between its barrier polls, which share that pipe with the atomics.
 //
 // Every mbarrier wait is bounded (MmaArgs::timeout_ns); on expiry the CTA
 // records KSTATUS_TIMEOUT, every other wait gives up, the last MMA drains
 // (bounded) and the TMEM is released.
 #include <cuda_runtime.h>
+#include <algorithm>
+#include <cmath>
 #include <cstdint>
 
 #include "dd_device.cuh"
@@ -78,6 +98,18 @@ constexpr unsigned kGenPollNs = 0;
 constexpr int kColsPerWarp = kN / (kEpiWarps / 4);  // columns of a tile each epilogue warp reads
 constexpr int kLoads = kColsPerWarp / 32;           // 32-column TMEM loads per warp and tile
 static_assert(kEpiWarps % 4 == 0 && kColsPerWarp % 32 == 0, "whole 32-column TMEM loads per warp and tile");
+// pair-packed epilogue
+constexpr int kPkHalf = kSuper / 2;                 // column p of a strip pairs with column p + 512
+constexpr int kPkTilesPerStrip = kPkHalf / kN;      // 2 MMA tiles of 256 packed columns per strip
+constexpr int kPkBBytes = kPkTilesPerStrip * kBTileBytes;  // 32 KB column operand per super tile
+constexpr uint32_t kPkFb = 64;                      // fallback row after the joint cells: single distances 0..63
+// Tiles between table flushes: a tile adds at most 16 warps x 64 values x 2
+// (an outlier counts twice in the fallback row) to a lane's column, so a
+// uint32 cell stays below 2^31 within 2^20 tiles.  (The 32 lane columns of a
+// cell can hold more than 2^32 together: the flush sums them in 64 bits.)
+constexpr uint32_t kPkFlushTiles = 1u << 20;
+template <bool kPk>
+__host__ __device__ constexpr int tiles_per_strip() { return kPk ? kPkTilesPerStrip : kTilesPerStrip; }
 __host__ __device__ constexpr uint32_t buf_of(uint64_t g) { return (uint32_t)(g % kBufs); }
 __host__ __device__ constexpr uint32_t parity_of(uint64_t g) { return (uint32_t)(g / kBufs) & 1u; }
 
@@ -190,6 +222,36 @@ __device__ __forceinline__ void put_chunk(uint8_t* base, int r, int c, uint4 v) 
   *reinterpret_cast<uint4*>(base + (r >> 3) * kSBO + c * kLBO + (r & 7) * 16) = v;
 }
 
+// Row (pair-packed epilogue) of codeword x with L bit planes: bytes -2*bit, then popc(x), S, 1.
+__device__ __forceinline__ void write_row_pk(uint8_t* base, int r, uint64_t x, int L, uint32_t S) {
+  uint32_t w[16];
+  const uint32_t pc = (uint32_t)popc64(x);
+#pragma unroll
+  for (int q = 0; q < 16; ++q) {
+    if (4 * q < L) w[q] = spread_nibble(x, q) * 0xFEu;
+    else if (4 * q == L) w[q] = pc | (S << 8) | (1u << 16);
+    else w[q] = 0;
+  }
+#pragma unroll
+  for (int c = 0; c < 4; ++c) put_chunk(base, r, c, make_uint4(w[4 * c], w[4 * c + 1], w[4 * c + 2], w[4 * c + 3]));
+}
+
+// Packed column of codewords y, y2 (pair-packed epilogue): bytes bit(y) + S*bit(y2)
+// (each <= S + 1 <= 127, no carries between bytes), then 1 + S, popc(y2) - lo, popc(y).
+__device__ __forceinline__ void write_col_pk(uint8_t* base, int r, uint64_t y, uint64_t y2, int L, uint32_t S,
+                                             int32_t lo) {
+  uint32_t w[16];
+  const uint32_t c1 = (uint32_t)popc64(y), c2 = (uint32_t)((int32_t)popc64(y2) - lo) & 0xFFu;
+#pragma unroll
+  for (int q = 0; q < 16; ++q) {
+    if (4 * q < L) w[q] = spread_nibble(y, q) + S * spread_nibble(y2, q);
+    else if (4 * q == L) w[q] = (1u + S) | (c2 << 8) | (c1 << 16);
+    else w[q] = 0;
+  }
+#pragma unroll
+  for (int c = 0; c < 4; ++c) put_chunk(base, r, c, make_uint4(w[4 * c], w[4 * c + 1], w[4 * c + 2], w[4 * c + 3]));
+}
+
 // Row/column operand of codeword x with L bit planes (L multiple of 4, L <= 60).
 // is_a: bytes -2*bit, then popc(x), 1;  else: bit, then 1, popc(x).
 __device__ __forceinline__ void write_operand(uint8_t* base, int r, uint64_t x, int L, bool is_a) {
@@ -256,6 +318,8 @@ struct Shared {
   StripInfo strip[2];
   uint64_t slot_full[2];  // strip ready: the generators' thread 0 arrives (count 1)
   uint64_t slot_free[2];  // every MMA of the strip done: tcgen05.commit after its last tile (count 1)
+  uint64_t epi_bar;       // pair-packed: epilogue-wide barrier around table flushes (count kEpiWarps)
+  unsigned long long sbins[kMaxBins];  // pair-packed: per-distance sums of one table flush
   uint32_t tmem_base;
   uint32_t abort;         // set by whichever wait ran out; every other wait then gives up too
   uint32_t gflag;         // generators: result of their thread 0's wait
@@ -300,34 +364,67 @@ __device__ __forceinline__ bool wait_or_abort(uint32_t addr, uint32_t parity, un
 }  // namespace
 
 // ---------------------------------------------------------------- kernel
+// Epilogue-wide barrier of the pair-packed epilogue (every epilogue warp, one
+// arrive each), bounded like every other wait; false once the CTA aborts.
+__device__ __forceinline__ bool epi_sync(Shared* sh, uint32_t& phase, int lane, unsigned long long timeout_ns,
+                                         volatile uint32_t* abort) {
+  __syncwarp();
+  bool r = true;
+  if (lane == 0) {
+    mbar_arrive(smem_u32(&sh->epi_bar));
+    r = wait_or_abort<kEpiPollNs>(smem_u32(&sh->epi_bar), phase, timeout_ns, abort);
+  }
+  phase ^= 1u;
+  const bool ok = __shfl_sync(0xffffffffu, r ? 1 : 0, 0) != 0;
+  __syncwarp();
+  return ok;
+}
+
+// Two single distances of a packed value (fallback row), for the outliers of
+// full tiles and the checked pairs of partial tiles: Q = P + S*lo = d1 + S*d2.
+__device__ __forceinline__ void pk_decode(uint32_t P, uint32_t S, int32_t lo, uint32_t& d1, uint32_t& d2) {
+  const uint32_t Q = P + S * (uint32_t)lo;
+  d2 = Q / S;
+  d1 = Q - d2 * S;
+}
+
 // Warp roles: warps 0..15 bin (epilogue), warp 16 issues the MMAs (lane 0),
 // warps 17..19 claim strips and write their operands.  Hand-offs go through
 // mbarriers only: slot_full/slot_free (a strip's operands written / its MMAs
 // done), full[b] (the MMA result in TMEM buffer b is ready, and for a strip's
 // first tile the strip's StripInfo),
-// empty[b] (all 16 epilogue warps have read buffer b).  No CTA-wide barrier
+// empty[b] (all 16 epilogue warps have read buffer b), and for the
+// pair-packed epilogue epi_bar around each table flush.  No CTA-wide barrier
 // runs between set-up and exit.
 //
 // Epilogue warp w reads TMEM lanes 32*(w%4).. (its rows) and 64 columns
-// 64*(w/4).. of each 256-column tile, and bumps one shared-memory counter per
-// pair in its own bin columns (row stride kEpiThreads words), so warps never
-// share a counter and each warp flushes its own columns.  A distance is at
-// most L (both operands have L bit planes, popc(x) <= L), and there are at
-// least L + 1 bin rows (mma_hist_rows), so it indexes the rows unchecked;
-// rows at or above the job's bin count are flagged at the flush.
+// 64*(w/4).. of each 256-column tile.  Single epilogue: it bumps one
+// shared-memory counter per pair in its own bin columns (row stride
+// kEpiThreads words), so warps never share a counter and each warp flushes its
+// own columns.  A distance is at most L (both operands have L bit planes,
+// popc(x) <= L), and there are at least L + 1 bin rows (mma_hist_rows), so it
+// indexes the rows unchecked; rows at or above the job's bin count are flagged
+// at the flush.  Pair-packed epilogue: one counter per packed value in the
+// joint table's column of its lane (see the file comment).
+template <bool kPk>
 __global__ void __launch_bounds__(kThreads, 1) mma_hist_kernel(MmaArgs args) {
+  constexpr int kTps = tiles_per_strip<kPk>();
+  constexpr int kColBytes = kPk ? kPkBBytes : kBBytes;  // column operand of one super tile
   extern __shared__ __align__(1024) uint8_t smem[];
-  // b_bufs x 64 KB: the column operand of a super tile (4 tiles of 256 columns), double-buffered
-  // when it fits, so the next super tile's operand is written while the current one's MMAs run
+  // b_bufs column operands of a super tile, double-buffered when they fit, so the
+  // next super tile's operand is written while the current one's MMAs run
   uint8_t* sB = smem;
-  uint8_t* sA = smem + (size_t)args.b_bufs * kBBytes;        // 2 x 8 KB: row operand, double-buffered by strip
-  uint32_t* hist = reinterpret_cast<uint32_t*>(sA + 2 * kABytes);  // hist_rows x kEpiThreads
-  Shared* sh = reinterpret_cast<Shared*>(sA + 2 * kABytes + (size_t)args.hist_rows * kEpiThreads * 4);
+  uint8_t* sA = smem + (size_t)args.b_bufs * kColBytes;       // 2 x 8 KB: row operand, double-buffered by strip
+  uint32_t* hist = reinterpret_cast<uint32_t*>(sA + 2 * kABytes);  // bins (single) or the joint table (packed)
+  // packed: pk_cells joint cells then the kPkFb fallback cells, one column per lane
+  const size_t hist_words = kPk ? (size_t)(args.pk_cells + kPkFb) * 32 : (size_t)args.hist_rows * kEpiThreads;
+  Shared* sh = reinterpret_cast<Shared*>(sA + 2 * kABytes + hist_words * 4);
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   volatile uint32_t* abort = &sh->abort;
 
-  for (uint32_t k = tid; k < args.hist_rows * kEpiThreads; k += kThreads) hist[k] = 0;
+  for (uint32_t k = tid; k < hist_words; k += kThreads) hist[k] = 0;
+  if (tid < kMaxBins) sh->sbins[tid] = 0;
   if (tid == 0) {
     for (int b = 0; b < kBufs; ++b) {
       mbar_init(smem_u32(&sh->full[b]), 2);
@@ -337,6 +434,7 @@ __global__ void __launch_bounds__(kThreads, 1) mma_hist_kernel(MmaArgs args) {
       mbar_init(smem_u32(&sh->slot_full[b]), 1);
       mbar_init(smem_u32(&sh->slot_free[b]), 1);
     }
+    mbar_init(smem_u32(&sh->epi_bar), kEpiWarps);
     sh->abort = 0;
     fence_mbar_init();
   }
@@ -412,6 +510,8 @@ __global__ void __launch_bounds__(kThreads, 1) mma_hist_kernel(MmaArgs args) {
         L = 64 - __clzll((long long)(maxcw | 1));
       }
       L = (L + 3) & ~3;
+      const uint32_t S = __ldg(&jp->pk_s);
+      const int32_t lo = __ldg(&jp->pk_lo);
       const uint32_t slot = (uint32_t)(s & 1);
       const bool need_b = jn != bjob || sc != bsc;
       // this slot's row operand may be rewritten once every MMA of strip s-2 is
@@ -433,12 +533,22 @@ __global__ void __launch_bounds__(kThreads, 1) mma_hist_kernel(MmaArgs args) {
       if (need_b) {
         bcur = args.b_bufs == 2 ? (bfill & 1u) : 0u;
         ++bfill;
-        uint8_t* bb = sB + (size_t)bcur * kBBytes;
+        uint8_t* bb = sB + (size_t)bcur * kColBytes;
+        const uint64_t ncols = rect ? NC : N;
+        if constexpr (kPk) {
+          // packed column p: columns c0 + p and c0 + p + 512 of the super tile
 #pragma unroll 1
-        for (int cc = gtid; cc < kSuper; cc += kGenThreads) {
-          const uint64_t j = c0 + cc;
-          write_operand(bb + (cc / kN) * kBTileBytes, cc % kN, j < (rect ? NC : N) ? mma_col_value(jp, j) : 0, L,
-                        false);
+          for (int cc = gtid; cc < kPkHalf; cc += kGenThreads) {
+            const uint64_t j = c0 + cc, j2 = j + kPkHalf;
+            write_col_pk(bb + (cc / kN) * kBTileBytes, cc % kN, j < ncols ? mma_col_value(jp, j) : 0,
+                         j2 < ncols ? mma_col_value(jp, j2) : 0, L, S, lo);
+          }
+        } else {
+#pragma unroll 1
+          for (int cc = gtid; cc < kSuper; cc += kGenThreads) {
+            const uint64_t j = c0 + cc;
+            write_operand(bb + (cc / kN) * kBTileBytes, cc % kN, j < ncols ? mma_col_value(jp, j) : 0, L, false);
+          }
         }
         bjob = jn;
         bsc = sc;
@@ -447,7 +557,9 @@ __global__ void __launch_bounds__(kThreads, 1) mma_hist_kernel(MmaArgs args) {
 #pragma unroll 1
       for (int rr = gtid; rr < kM; rr += kGenThreads) {
         const uint64_t i = r0 + rr;
-        write_operand(a, rr, i < N ? mma_row_value(jp, i) : 0, L, true);
+        const uint64_t x = i < N ? mma_row_value(jp, i) : 0;
+        if constexpr (kPk) write_row_pk(a, rr, x, L, S);
+        else write_operand(a, rr, x, L, true);
       }
       fence_proxy_async();
       gen_bar();  // both operands complete
@@ -477,7 +589,7 @@ __global__ void __launch_bounds__(kThreads, 1) mma_hist_kernel(MmaArgs args) {
     if (lane == 0) {
       uint64_t g = 0;  // tiles issued
       bool normal = false;
-      // until the epilogue has read tile gg-4, the previous tile of gg's buffer
+      // until the epilogue has read tile gg-kBufs, the previous tile of gg's buffer
       auto wait_empty = [&](uint64_t gg) -> bool {
         return gg < kBufs ||
                wait_or_abort<kIssuerPollNs>(smem_u32(&sh->empty[buf_of(gg)]), parity_of(gg - kBufs), args.timeout_ns,
@@ -490,18 +602,19 @@ __global__ void __launch_bounds__(kThreads, 1) mma_hist_kernel(MmaArgs args) {
         if (si.flags & kInfoDone) { normal = true; break; }
         const uint32_t a0 = smem_u32(sA + slot * kABytes);
         bool ok = true;
-        for (int tile = 0; tile < kTilesPerStrip; ++tile, ++g) {
+        for (int tile = 0; tile < kTps; ++tile, ++g) {
           if (!wait_empty(g)) { ok = false; break; }
           const uint32_t b = buf_of(g);
           if (tile == 0) {
-            // the entry of strip s-2: every warp read it at tile g-16 < g-4
-            StripInfo& es = sh->estrip[(g / kTilesPerStrip) & 1];
+            // the entry of strip s-2: every warp read it at tile g-2*kTps, before
+            // tile g-kBufs, which wait_empty has seen read
+            StripInfo& es = sh->estrip[(g / kTps) & 1];
             es = si;
             es.flags = si.flags & (kInfoFull | kInfoRect);
           }
           tc_fence_after();
           const uint32_t d = tmem + b * (uint32_t)kN;
-          const uint32_t b0 = smem_u32(sB + (size_t)si.bbuf * kBBytes + tile * kBTileBytes);
+          const uint32_t b0 = smem_u32(sB + (size_t)si.bbuf * kColBytes + tile * kBTileBytes);
 #pragma unroll
           for (int ks = 0; ks < kK / 32; ++ks)  // K = 32 bytes per instruction = 2 core matrices
             mma_i8(d, smem_desc(a0 + ks * 2 * kLBO), smem_desc(b0 + ks * 2 * kLBO), ks > 0 ? 1u : 0u);
@@ -513,7 +626,7 @@ __global__ void __launch_bounds__(kThreads, 1) mma_hist_kernel(MmaArgs args) {
       }
       if (normal && wait_empty(g)) {
         // end of work: a strip marked done wakes the epilogue warps (g is a strip's first tile)
-        sh->estrip[(g / kTilesPerStrip) & 1].flags = kInfoDone;
+        sh->estrip[(g / kTps) & 1].flags = kInfoDone;
         mbar_arrive(smem_u32(&sh->full[buf_of(g)]));
         mbar_arrive(smem_u32(&sh->full[buf_of(g)]));
       } else {
@@ -527,11 +640,15 @@ __global__ void __launch_bounds__(kThreads, 1) mma_hist_kernel(MmaArgs args) {
   } else {
     // ------------------------------------------------------------ epilogue
     const int q = warp & 3, sub = warp >> 2;
-    const uint32_t hist_lane = smem_u32(hist) + (uint32_t)tid * 4u;
     uint32_t cur = 0xffffffffu, nbins = 0, since_flush = 0;
     unsigned long long* bins = nullptr;
     bool ok = true;
-    // this warp's bin columns -> the job's global bins
+    // pair-packed state: the table's column of this lane, the current job's S and window
+    const uint32_t pk_lane = smem_u32(hist) + (uint32_t)lane * 4u;
+    const uint32_t pk_fb = pk_lane + (args.pk_cells << 7);
+    uint32_t pkS = 1, pklimit = 0, epi_phase = 0;
+    int32_t pklo = 0;
+    // single: this warp's bin columns -> the job's global bins
     auto flush = [&]() {
       for (uint32_t b = 0; b < args.hist_rows; ++b) {
         const uint32_t x = hist[b * kEpiThreads + tid];
@@ -543,6 +660,52 @@ __global__ void __launch_bounds__(kThreads, 1) mma_hist_kernel(MmaArgs args) {
         }
       }
     };
+    // pair-packed: every epilogue warp folds a share of the table's cells into the
+    // flush sums (a joint cell adds to d1 and to d2), then warp 0 adds the sums to
+    // the job's bins.  False once the CTA aborted.
+    auto flush_pk = [&]() -> bool {
+      if (!epi_sync(sh, epi_phase, lane, args.timeout_ns, abort)) return false;
+      for (uint32_t c = (uint32_t)warp; c < args.pk_cells + kPkFb; c += kEpiWarps) {
+        const uint32_t x = hist[c * 32 + lane];
+        hist[c * 32 + lane] = 0;
+        // 32 cells of up to 2^31 each: reduce the 16-bit halves, sum in 64 bits
+        const unsigned long long s = (unsigned long long)__reduce_add_sync(0xffffffffu, x & 0xFFFFu) +
+                                     ((unsigned long long)__reduce_add_sync(0xffffffffu, x >> 16) << 16);
+        if (lane == 0 && s) {
+          if (c < args.pk_cells) {
+            const uint32_t d1 = c % pkS, d2 = c / pkS + (uint32_t)pklo;
+            atomicAdd(&sh->sbins[d1], s);
+            if (d2 < (uint32_t)kMaxBins) atomicAdd(&sh->sbins[d2], s);
+            else atomicOr(args.status, KSTATUS_BAD_DISTANCE);
+          } else {
+            atomicAdd(&sh->sbins[c - args.pk_cells], s);
+          }
+        }
+      }
+      if (!epi_sync(sh, epi_phase, lane, args.timeout_ns, abort)) return false;
+      if (warp == 0) {
+        for (uint32_t d = (uint32_t)lane; d < (uint32_t)kMaxBins; d += 32) {
+          const unsigned long long v = sh->sbins[d];
+          sh->sbins[d] = 0;
+          if (v) {
+            if (d < nbins) atomicAdd(bins + d, v);
+            else atomicOr(args.status, KSTATUS_BAD_DISTANCE);
+          }
+        }
+      }
+      return true;
+    };
+    // pair-packed: one packed value counted as two single distances (fallback row)
+    auto pk_single = [&](uint32_t P, bool v1, bool v2) {
+      uint32_t d1, d2;
+      pk_decode(P, pkS, pklo, d1, d2);
+      if (d2 >= kPkFb) {  // not a value the operands can produce
+        atomicOr(args.status, KSTATUS_BAD_DISTANCE);
+        return;
+      }
+      if (v1) red_shared(pk_fb + (d1 << 7));
+      if (v2) red_shared(pk_fb + (d2 << 7));
+    };
     unsigned long long r0 = 0, cs = 0, n = 0, nc = 0;  // the current strip: first row and column, rows, columns
     uint32_t flags = 0, job = 0;
     for (uint64_t g = 0;; ++g) {
@@ -551,9 +714,9 @@ __global__ void __launch_bounds__(kThreads, 1) mma_hist_kernel(MmaArgs args) {
       if (lane == 0) r = wait_or_abort<kEpiPollNs>(smem_u32(&sh->full[b]), parity_of(g), args.timeout_ns, abort);
       if (!__shfl_sync(0xffffffffu, r ? 1 : 0, 0)) { ok = false; break; }
       __syncwarp();  // lane 0's wait acquired the MMA result (and StripInfo); this orders it for the warp
-      const uint32_t tile = (uint32_t)(g % kTilesPerStrip);
+      const uint32_t tile = (uint32_t)(g % kTps);
       if (tile == 0) {
-        const StripInfo& es = sh->estrip[(g / kTilesPerStrip) & 1];
+        const StripInfo& es = sh->estrip[(g / kTps) & 1];
         flags = es.flags;
         if (flags & kInfoDone) break;
         job = es.job;
@@ -562,45 +725,116 @@ __global__ void __launch_bounds__(kThreads, 1) mma_hist_kernel(MmaArgs args) {
         n = es.n;
         nc = es.cols;
       }
+      if constexpr (kPk) {
+        // a new job: the table must hold one job's counts, so every warp folds it
+        // first (all warps see the same strips, so they flush at the same tile)
+        if (job != cur) {
+          if (cur != 0xffffffffu && !flush_pk()) { ok = false; break; }
+          since_flush = 0;
+          cur = job;
+          bins = args.jobs[job].bins;
+          nbins = args.jobs[job].nbins;
+          pkS = args.jobs[job].pk_s;
+          pklo = args.jobs[job].pk_lo;
+          pklimit = args.jobs[job].pk_limit;  // <= pk_cells (host)
+        }
+      }
       tc_fence_after();
       uint32_t v[kLoads][32];
 #pragma unroll
       for (int h = 0; h < kLoads; ++h)
         tmem_ld32_nowait(tmem + ((uint32_t)(q * 32) << 16) + b * (uint32_t)kN + (uint32_t)(sub * kColsPerWarp + 32 * h),
                          v[h]);
-      const unsigned long long c0 = cs + (unsigned long long)tile * kN;
       tmem_wait_ld();
       // the buffer may be refilled as soon as every warp has its values in registers
       tc_fence_before();
       __syncwarp();
       if (lane == 0) mbar_arrive(smem_u32(&sh->empty[b]));
-      if (job != cur) {
-        if (cur != 0xffffffffu && since_flush) flush();
-        since_flush = 0;
-        cur = job;
-        bins = args.jobs[job].bins;
-        nbins = args.jobs[job].nbins;
-      }
-      if (flags & kInfoFull) {
+      if constexpr (kPk) {
+        if (flags & kInfoFull) {
+          // one unsigned max over the tile's values tests every d2 against the
+          // window at once (a d2 below it gives a negative value, i.e. a huge
+          // one); taken as a tree of depth 6, not a chain of 64 dependent maxima:
+          // every epilogue warp reaches this point at the same time
+          static_assert(kLoads == 2, "the max tree takes two 32-value loads");
+          uint32_t m[16];
 #pragma unroll
-        for (int h = 0; h < kLoads; ++h)
+          for (int u = 0; u < 16; ++u)
+            m[u] = max(max(v[0][2 * u], v[0][2 * u + 1]), max(v[1][2 * u], v[1][2 * u + 1]));
 #pragma unroll
-          for (int u = 0; u < 32; ++u) red_shared(hist_lane + (v[h][u] << 11));
-      } else {
-        const uint64_t i = r0 + (uint64_t)(q * 32 + lane);
-        const uint64_t j0 = c0 + (uint64_t)(sub * kColsPerWarp);
+          for (int w = 8; w >= 1; w >>= 1)
 #pragma unroll
-        for (int h = 0; h < kLoads; ++h)
+            for (int u = 0; u < w; ++u) m[u] = max(m[u], m[u + w]);
+          if (__any_sync(0xffffffffu, m[0] >= pklimit)) {
+            // some d2 outside the window: those values count as two single distances
 #pragma unroll
-          for (int u = 0; u < 32; ++u) {
-            const uint64_t j = j0 + 32 * h + u;
-            const bool in = (flags & kInfoRect) ? (i < n && j < nc) : (i < n && j < n && j > i);
-            if (in) red_shared(hist_lane + (v[h][u] << 11));
+            for (int h = 0; h < kLoads; ++h)
+#pragma unroll
+              for (int u = 0; u < 32; ++u) {
+                if (v[h][u] < pklimit) red_shared(pk_lane + (v[h][u] << 7));
+                else pk_single(v[h][u], true, true);
+              }
+          } else {
+#pragma unroll
+            for (int h = 0; h < kLoads; ++h)
+#pragma unroll
+              for (int u = 0; u < 32; ++u) red_shared(pk_lane + (v[h][u] << 7));
           }
+        } else {
+          // partial strip: every pair checked, counted singly
+          const uint64_t i = r0 + (uint64_t)(q * 32 + lane);
+          const uint64_t j0 = cs + (uint64_t)tile * kN + (uint64_t)(sub * kColsPerWarp);
+          // fully unrolled: the values stay in registers (a loop index into v[][]
+          // would move the array to local memory)
+#pragma unroll
+          for (int h = 0; h < kLoads; ++h)
+#pragma unroll
+            for (int u = 0; u < 32; ++u) {
+              const uint64_t j = j0 + 32 * h + u, j2 = j + kPkHalf;
+              const bool v1 = (flags & kInfoRect) ? (i < n && j < nc) : (i < n && j < n && j > i);
+              const bool v2 = (flags & kInfoRect) ? (i < n && j2 < nc) : (i < n && j2 < n && j2 > i);
+              if (v1 || v2) pk_single(v[h][u], v1, v2);
+            }
+        }
+        if (++since_flush >= kPkFlushTiles) {
+          if (!flush_pk()) { ok = false; break; }
+          since_flush = 0;
+        }
+      } else {
+        if (job != cur) {
+          if (cur != 0xffffffffu && since_flush) flush();
+          since_flush = 0;
+          cur = job;
+          bins = args.jobs[job].bins;
+          nbins = args.jobs[job].nbins;
+        }
+        const uint32_t hist_lane = smem_u32(hist) + (uint32_t)tid * 4u;
+        if (flags & kInfoFull) {
+#pragma unroll
+          for (int h = 0; h < kLoads; ++h)
+#pragma unroll
+            for (int u = 0; u < 32; ++u) red_shared(hist_lane + (v[h][u] << 11));
+        } else {
+          const unsigned long long c0 = cs + (unsigned long long)tile * kN;
+          const uint64_t i = r0 + (uint64_t)(q * 32 + lane);
+          const uint64_t j0 = c0 + (uint64_t)(sub * kColsPerWarp);
+#pragma unroll
+          for (int h = 0; h < kLoads; ++h)
+#pragma unroll
+            for (int u = 0; u < 32; ++u) {
+              const uint64_t j = j0 + 32 * h + u;
+              const bool in = (flags & kInfoRect) ? (i < n && j < nc) : (i < n && j < n && j > i);
+              if (in) red_shared(hist_lane + (v[h][u] << 11));
+            }
+        }
+        if (++since_flush >= kFlushEvery) { flush(); since_flush = 0; }
       }
-      if (++since_flush >= kFlushEvery) { flush(); since_flush = 0; }
     }
-    if (ok && cur != 0xffffffffu && since_flush) flush();
+    if constexpr (kPk) {
+      if (ok && cur != 0xffffffffu) flush_pk();
+    } else {
+      if (ok && cur != 0xffffffffu && since_flush) flush();
+    }
   }
   tc_fence_before();
   __syncthreads();
@@ -611,18 +845,89 @@ __global__ void __launch_bounds__(kThreads, 1) mma_hist_kernel(MmaArgs args) {
 }
 
 // ---------------------------------------------------------------- host side
+int mma_max_distance(const Job& j) {
+  if (j.row_kind == ROW_HAMMING_EXT) return (int)j.nbins - 1;  // extended Hamming codeword: n data + h check bits
+  const unsigned __int128 maxcw = (unsigned __int128)j.A * ((1ull << j.n) - 1ull);
+  int bits = 0;
+  for (unsigned __int128 v = maxcw; v; v >>= 1) ++bits;
+  return bits ? bits : 1;
+}
+
 // Bit planes of the operands of job j: the bits of A * (2^n - 1), which bounds
 // every codeword of the job, rounded up to 4 (the kernel computes the same).
-int mma_operand_bits(const Job& j) {
-  int bits = 0;
-  if (j.row_kind == ROW_HAMMING_EXT) {
-    bits = (int)j.nbins - 1;  // extended Hamming codeword: n data + h check bits
-  } else {
-    const unsigned __int128 maxcw = (unsigned __int128)j.A * ((1ull << j.n) - 1ull);
-    for (unsigned __int128 v = maxcw; v; v >>= 1) ++bits;
-    if (bits == 0) bits = 1;
+int mma_operand_bits(const Job& j) { return (mma_max_distance(j) + 3) & ~3; }
+
+static uint64_t host_row_value(const Job& j, uint64_t i) {
+  switch (j.row_kind) {
+    case ROW_LATTICE: return lattice_value(j.A, i, j.row_step, j.t32);
+    case ROW_HAMMING_EXT: return hamming_cw_ext(i, j.n);
+    default: return j.A * i;
   }
-  return (bits + 3) & ~3;
+}
+static uint64_t host_col_value(const Job& j, uint64_t c) {
+  switch (j.col_kind) {
+    case COL_LATTICE: return lattice_value(j.A, c, j.col_step, j.t32);
+    case COL_HAMMING_EXT: return hamming_cw_ext(c, j.n);
+    default: return j.A * c;
+  }
+}
+
+// Shared memory beside the joint table: the row operand (two strips), the
+// column operand buffers, the Shared block and alignment slack.
+static size_t pk_fixed_bytes(uint32_t b_bufs) {
+  return (size_t)2 * kABytes + (size_t)b_bufs * kPkBBytes + sizeof(Shared) + 64;
+}
+
+static size_t smem_optin() {
+  int dev = 0, optin = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess)
+    return 227 * 1024;
+  return (size_t)optin;
+}
+
+void mma_pk_layout(uint32_t smax, uint32_t* cells, uint32_t* b_bufs) {
+  const size_t optin = smem_optin();
+  const size_t want = (size_t)smax * smax;
+  auto fit = [&](uint32_t bufs) -> size_t {  // joint cells that fit beside `bufs` column buffers
+    const size_t fixed = pk_fixed_bytes(bufs) + (size_t)kPkFb * 128;
+    return optin > fixed ? (optin - fixed) / 128 : 0;
+  };
+  if (want <= fit(2)) {
+    *cells = (uint32_t)want;
+    *b_bufs = 2;
+  } else {
+    *cells = (uint32_t)std::min(want, fit(1));
+    *b_bufs = 1;
+  }
+}
+
+void mma_pack_setup(Job& j, uint32_t cells) {
+  const uint32_t S = (uint32_t)mma_max_distance(j) + 1u;
+  uint32_t rows = cells / S;  // whole rows of S cells: d2 - lo in [0, rows)
+  if (rows > S) rows = S;
+  int32_t lo = 0;
+  if (rows < S && j.rows && j.cols) {
+    // mean distance of 512 pairs drawn by a fixed generator (the same job always
+    // gets the same window, so a cached launch graph stays valid)
+    uint64_t st = 0x9E3779B97F4A7C15ull ^ (j.A * 0xBF58476D1CE4E5B9ull) ^ ((uint64_t)j.n << 56) ^ j.rows;
+    auto next = [&st]() {
+      st ^= st << 13; st ^= st >> 7; st ^= st << 17;
+      return st;
+    };
+    double sum = 0;
+    const int kSamples = 512;
+    for (int k = 0; k < kSamples; ++k) {
+      const uint64_t i = next() % j.rows, c = next() % j.cols;
+      sum += (double)popc64(host_row_value(j, i) ^ host_col_value(j, c));
+    }
+    lo = (int32_t)std::lround(sum / kSamples - (double)(rows - 1) / 2.0);
+    if (lo > (int32_t)(S - rows)) lo = (int32_t)(S - rows);
+    if (lo < 0) lo = 0;
+  }
+  j.pk_s = S;
+  j.pk_lo = lo;
+  j.pk_limit = S * rows;
 }
 
 bool mma_eligible(const Job& j) {
@@ -634,23 +939,38 @@ bool mma_eligible(const Job& j) {
   return (tri || rect) && mma_operand_bits(j) <= 60;
 }
 
-size_t mma_smem_bytes(uint32_t hist_rows, uint32_t b_bufs) {
-  size_t s = (size_t)2 * kABytes + (size_t)b_bufs * kBBytes + (size_t)hist_rows * kEpiThreads * 4 + sizeof(Shared) + 64;
+size_t mma_smem_bytes(uint32_t hist_rows, uint32_t b_bufs, bool packed, uint32_t pk_cells) {
+  size_t s;
+  if (packed) {
+    s = pk_fixed_bytes(b_bufs) + ((size_t)pk_cells + kPkFb) * 128;
+  } else {
+    s = (size_t)2 * kABytes + (size_t)b_bufs * kBBytes + (size_t)hist_rows * kEpiThreads * 4 + sizeof(Shared) + 64;
+  }
   return s < kMinSmem ? kMinSmem : s;
 }
 
 uint32_t mma_b_bufs(uint32_t hist_rows) {
-  int dev = 0, optin = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess ||
-      cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess)
-    return 1;
-  return mma_smem_bytes(hist_rows, 2) <= (size_t)optin ? 2u : 1u;
+  return mma_smem_bytes(hist_rows, 2, false, 0) <= smem_optin() ? 2u : 1u;
 }
 
 cudaError_t launch_mma(const MmaArgs& args, int grid, size_t smem, cudaStream_t stream) {
-  cudaError_t e = cudaFuncSetAttribute(mma_hist_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  // the per-function limit is process-wide: every caller sets the same value
+  // (the device's opt-in maximum), so host threads launching plans of different
+  // sizes cannot lower it under one another
+  int dev = 0, optin = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
   if (e != cudaSuccess) return e;
-  mma_hist_kernel<<<grid, kThreads, smem, stream>>>(args);
+  if (smem > (size_t)optin) return cudaErrorInvalidValue;
+  if (args.packed) {
+    e = cudaFuncSetAttribute(mma_hist_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
+    if (e != cudaSuccess) return e;
+    mma_hist_kernel<true><<<grid, kThreads, smem, stream>>>(args);
+  } else {
+    e = cudaFuncSetAttribute(mma_hist_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
+    if (e != cudaSuccess) return e;
+    mma_hist_kernel<false><<<grid, kThreads, smem, stream>>>(args);
+  }
   return cudaGetLastError();
 }
 

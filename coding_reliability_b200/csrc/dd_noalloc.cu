@@ -10,11 +10,13 @@
 //
 // Here that scratch lives in one file-scope __device__ array of fixed size,
 // present on every GPU that loads the library until the process exits.  The
-// host code below never names the array as a device address: on the first call
-// on a device, with that device current, it asks the runtime for the array's
-// address (cudaGetSymbolAddress) and passes that pointer to the kernel.  The
-// first call on a device therefore does this set-up and should come before any
-// stream capture on that device.
+// host code below never names the array as a device address: on every call,
+// with the caller's device current, it asks the runtime for the array's address
+// on that device (cudaGetSymbolAddress) and passes that pointer to the kernel.
+// The lookup is not cached, so a context that was reset and re-created between
+// calls gets the address of its own copy of the array.  The first call on a
+// device also loads the module there, so it should come before any stream
+// capture on that device.  The caller's current device is restored on return.
 //
 // Limits and sharing:
 //   - at most kNoAllocMaxRequests requests per call (bins, job table and
@@ -29,7 +31,6 @@
 
 #include <chrono>
 #include <cstring>
-#include <mutex>
 #include <string>
 #include <vector>
 
@@ -53,24 +54,33 @@ struct NoAllocScratch {
 static __device__ __align__(256) unsigned char g_noalloc_scratch[sizeof(NoAllocScratch)];
 
 constexpr int kMaxDevices = 64;
-std::mutex g_setup_mu;
-NoAllocScratch* g_scratch[kMaxDevices] = {nullptr};
 
-// Device address of the scratch array on `device` (current), looked up once.
-int scratch_on(int device, NoAllocScratch** out) {
-  std::lock_guard<std::mutex> lk(g_setup_mu);
-  if (!g_scratch[device]) {
-    void* p = nullptr;
-    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    if (e != cudaSuccess) {
-      set_error(std::string("dd_histogram_noalloc: cudaGetSymbolAddress: ") + cudaGetErrorString(e));
-      return DD_ERR_CUDA;
-    }
-    g_scratch[device] = static_cast<NoAllocScratch*>(p);
+// Device address of the scratch array on the current device.
+int scratch_here(NoAllocScratch** out) {
+  void* p = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+  if (e != cudaSuccess) {
+    set_error(std::string("dd_histogram_noalloc: cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+    return DD_ERR_CUDA;
   }
-  *out = g_scratch[device];
+  *out = static_cast<NoAllocScratch*>(p);
   return DD_OK;
 }
+
+// Makes `device` current for the call and gives the caller's device back on
+// every return path.
+struct DeviceGuard {
+  int saved = -1;
+  cudaError_t enter(int device) {
+    cudaError_t e = cudaGetDevice(&saved);
+    if (e != cudaSuccess) { saved = -1; return e; }
+    return saved == device ? cudaSuccess : cudaSetDevice(device);
+  }
+  ~DeviceGuard() {
+    int cur = -1;
+    if (saved >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != saved) cudaSetDevice(saved);
+  }
+};
 
 }  // namespace
 }  // namespace dd
@@ -93,13 +103,14 @@ extern "C" int dd_histogram_noalloc(int device, void* stream, const dd_request* 
   }
   const auto t0 = std::chrono::steady_clock::now();
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  cudaError_t e = cudaSetDevice(device);
+  DeviceGuard guard;
+  cudaError_t e = guard.enter(device);
   if (e != cudaSuccess) {
     set_error(std::string("dd_histogram_noalloc: cudaSetDevice: ") + cudaGetErrorString(e));
     return DD_ERR_NO_DEVICE;
   }
   NoAllocScratch* scratch = nullptr;
-  int st = scratch_on(device, &scratch);
+  int st = scratch_here(&scratch);
   if (st != DD_OK) return st;
 
   // plan: one popc-path job per request, bins slot = request index

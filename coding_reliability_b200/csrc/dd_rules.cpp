@@ -266,6 +266,9 @@ u128 planned_pairs(const Shape& s, const dd_request& req) {
 // ---------------------------------------------------------------------------
 static void store128(u128 v, uint64_t& lo, uint64_t& hi) { lo = (uint64_t)v; hi = (uint64_t)(v >> 64); }
 
+// res.raw receives raw_in unchanged: the device bins of every evaluated pair,
+// whatever the entry point (dd_histogram, the sum of dd_histogram_part calls,
+// a query server slot).  Conventions that drop bins apply to counts only.
 void postprocess(const dd_request& req, const Shape& s, const uint64_t* raw_in, dd_result& res) {
   uint64_t raw[kMaxBins + 1] = {0};
   for (uint32_t i = 0; i < s.nbins; ++i) raw[i] = raw_in[i];
@@ -279,7 +282,9 @@ void postprocess(const dd_request& req, const Shape& s, const uint64_t* raw_in, 
       c[0] = (u128)1 << n;
       for (uint32_t i = 1; i < nb; ++i) c[i] = (u128)raw[i] << 1;
     } else if (s.mode == DD_MODE_GRID_1D || s.mode == DD_MODE_GRID_2D) {
-      if (s.mode == DD_MODE_GRID_2D) raw[0] = 0;  // dancoding_grid_2d never flushes bin 0
+      // dancoding_grid_2d never flushes bin 0 (an_coding_grid.cu:121-140): the
+      // coincident lattice points the device counted there are left out of counts
+      if (s.mode == DD_MODE_GRID_2D) raw[0] = 0;
       // an_coding_grid.cu:316-322
       const long double factor = s.mode == DD_MODE_GRID_1D
                                      ? powl(2.0L, (long double)n) / s.m
@@ -352,7 +357,7 @@ void postprocess(const dd_request& req, const Shape& s, const uint64_t* raw_in, 
   res.iterations = s.m;
   res.iterations2 = s.mode == DD_MODE_GRID_2D ? s.m2 : 0;
   for (uint32_t i = 0; i < kMaxBins; ++i) {
-    res.raw[i] = i < nb ? raw[i] : 0;
+    res.raw[i] = i < nb ? raw_in[i] : 0;
     store128(i < nb ? c[i] : 0, res.counts_lo[i], res.counts_hi[i]);
   }
 }

@@ -208,6 +208,7 @@ void scheduler(dd_server* s) {
       q.result.pairs_hi = (uint64_t)(q.pairs >> 64);
       q.result.kernel_used = s->ctx ? (dd::uses_mma(s->ctx, q.job, q.req.kernel) ? DD_KERNEL_MMA : DD_KERNEL_POPC)
                                     : 0xFFFFFFFFu;
+      q.result.mma_epilogue = q.result.kernel_used == DD_KERNEL_MMA ? dd::mma_epilogue_used(s->ctx) : 0u;
       q.result.kernel_ms = ms;
       finish(s, q, DD_OK);
     }
@@ -245,6 +246,10 @@ int dd_server_create(int device, const dd_server_options* opts, dd_server** out)
   if (!s->opt.dry_run) {
     int st = dd_context_create(device, nullptr, &s->ctx);
     if (st != DD_OK) { delete s; return st; }
+    // KERNEL_AUTO queries run on the kernel the autotuner measures fastest on this
+    // GPU (about a second, once per server)
+    st = dd_autotune(s->ctx, nullptr);
+    if (st != DD_OK) { dd_context_destroy(s->ctx); delete s; return st; }
     const cudaError_t e = cudaMalloc(&s->d_slots, (size_t)s->nslots * dd::kMaxBins * 8);
     if (e != cudaSuccess) {
       dd_context_destroy(s->ctx);

@@ -73,6 +73,14 @@ typedef enum dd_kernel {
   DD_KERNEL_MMA = 2    /* tcgen05 kind::i8 bit-plane MMA, histogram epilogue from TMEM */
 } dd_kernel;
 
+/* Histogram epilogue of the tcgen05 kernel (dd_set_mma_epilogue). */
+typedef enum dd_mma_epilogue {
+  DD_MMA_EPILOGUE_AUTO = 0,    /* the autotuner's choice (paired until it has run) */
+  DD_MMA_EPILOGUE_PAIRED = 1,  /* two codewords per MMA column: the accumulator is a packed distance
+                                  pair, one shared-memory atomic per two pairs into a joint-bin table */
+  DD_MMA_EPILOGUE_SINGLE = 2   /* one codeword per MMA column: one atomic per pair, per-thread bins */
+} dd_mma_epilogue;
+
 /* Ext-Hamming exhaustive algorithm (reference `-e` switch, src/main.cpp:245-268). */
 typedef enum dd_hamming_method {
   DD_HAMMING_WEIGHTS = 0,   /* `-e 1`: weight enumerator x 2^n (src/hamming.cu:64-224) */
@@ -117,7 +125,9 @@ typedef struct dd_result {
   uint64_t iterations;      /* m after capping at 2^n (grid / MC), else 0 */
   uint64_t iterations2;     /* m2 after capping (2-D grid), else 0 */
   uint64_t pairs_lo, pairs_hi;  /* distance evaluations the device performed (uint128) */
-  uint64_t raw[DD_MAX_BINS];    /* device histogram: the reference's host-summed hcounts[0][] */
+  uint64_t raw[DD_MAX_BINS];    /* device histogram of every evaluated pair (the reference's host-summed
+                                   hcounts[0][]); 2-D grids: bin 0 holds the coincident lattice points,
+                                   which dancoding_grid_2d never flushes and counts[0] leaves out */
   uint64_t counts_lo[DD_MAX_BINS];  /* post-processed uint128 counts[] (lo 64 bits) */
   uint64_t counts_hi[DD_MAX_BINS];  /*                                  (hi 64 bits) */
   uint64_t minb;            /* first non-zero bin in the convention's range, 0xFFFF if none */
@@ -127,6 +137,8 @@ typedef struct dd_result {
   double kernel_ms;         /* device time of the histogram kernel(s), CUDA events */
   double total_ms;          /* host wall time of the whole call */
   uint64_t user_tag;
+  uint32_t mma_epilogue;    /* dd_mma_epilogue that ran when kernel_used is DD_KERNEL_MMA, else 0 */
+  uint32_t reserved;
 } dd_result;
 
 typedef struct dd_context dd_context;
@@ -182,11 +194,13 @@ int dd_histogram_plain(dd_context* ctx, const dd_request* req, dd_result* res);
  * or any allocating routine.  The kernel's scratch (bins, job table, work
  * counter, status word) is one fixed 21 KB __device__ array that every GPU
  * loading the library holds until exit; more than 32 requests per call are
- * refused with DD_ERR_INVALID_ARGUMENT.  The first call on a device looks up
- * the array's device address and should come before any stream capture on that
- * device.  All calls share the array: calls that overlap on the GPU race and
- * must be serialised by the caller.  Results equal dd_histogram's; kernel_ms
- * is 0 (no events are created). */
+ * refused with DD_ERR_INVALID_ARGUMENT.  Every call looks up the array's
+ * device address on `device`; the first call on a device also loads the
+ * module there and should come before any stream capture on that device.  The
+ * caller's current device is restored before the call returns.  All calls
+ * share the array: calls that overlap on the GPU race and must be serialised
+ * by the caller.  Results equal dd_histogram's; kernel_ms is 0 (no events are
+ * created). */
 int dd_histogram_noalloc(int device, void* stream, const dd_request* reqs, uint32_t count, dd_result* results);
 
 /* Monte Carlo continued (AN codes): the result of `req` (req->m samples per
@@ -222,6 +236,8 @@ int dd_batch_run(dd_context* ctx, const dd_request* reqs, uint32_t count,
  * while others run join the next round and their work overlaps on the GPU.
  * Queries beyond the slots wait in a bounded queue; beyond the queue,
  * dd_server_submit returns DD_ERR_BUSY.  Results are identical to dd_histogram's.
+ * dd_server_create runs the autotuner on the server's own context (about a
+ * second), so KERNEL_AUTO queries run on the kernel measured fastest there.
  * No counterpart in the reference (its drivers run one query per process). */
 typedef struct dd_server dd_server;
 
@@ -289,23 +305,46 @@ typedef struct dd_tuning {
   uint32_t hist_mode;         /* popc path bin increment: 0 = red.shared.add, 1 = load/add/store */
   double popc_red_pairs_per_s;
   double popc_ldst_pairs_per_s;
-  double mma_pairs_per_s;
+  double mma_pairs_per_s;     /* tcgen05, single epilogue */
   uint64_t probe_pairs;       /* pairs of the probe instance each variant ran */
+  double mma_paired_pairs_per_s;  /* tcgen05, paired epilogue */
+  uint32_t mma_epilogue;      /* dd_mma_epilogue chosen for the tcgen05 kernel */
+  uint32_t reserved;
 } dd_tuning;
 
-/* Times every kernel variant on a probe instance (A = 65521, k = 20: 36-bit
- * codewords, 5.5e11 pairs, about a second in all) on this context's GPU and
- * keeps the fastest for kernel = AUTO.  Runs by itself before the first large
- * AUTO request. */
+/* Times every kernel variant (popc with either bin increment, tcgen05 with
+ * either epilogue) on a probe instance (A = 65521, k = 20: 36-bit codewords,
+ * 5.5e11 pairs, about a second in all) on this context's GPU and keeps the
+ * fastest for kernel = AUTO, and the faster tcgen05 epilogue for the
+ * tcgen05 kernel.  Runs by itself before the first large AUTO request. */
 int dd_autotune(dd_context* ctx, dd_tuning* out);
+
+/* Epilogue of this context's tcgen05 launches (dd_mma_epilogue): AUTO follows
+ * the autotuner; PAIRED and SINGLE fix it (for measurements and tests).  Both
+ * give the identical histogram. */
+int dd_set_mma_epilogue(dd_context* ctx, uint32_t epilogue);
 
 /* --- measurement -------------------------------------------------------- */
 /* Measures the device's POPC issue rate (popc/s) with a dependency-free POPC
  * loop on the context's stream. */
 int dd_measure_popc_peak(dd_context* ctx, double* popc_per_s);
-/* Measures the device's shared-memory atomic rate (red.shared.add.u32 per
- * second, conflict-free, 16 warps per SM): the bound of the tcgen05 path's
- * histogram epilogue, one atomic per distance. */
+/* One point of the shared-memory atomic sweep: red.shared.add.u32 per second
+ * on every SM, one CTA of warps_per_sm warps each, 32 independent adds per
+ * loop iteration, conflict-free within each warp.  pattern 0: every thread
+ * its own column of 32 rows (the single tcgen05 epilogue's bins); pattern 1:
+ * one column per lane shared by every warp of the CTA, 1024 cells (the paired
+ * epilogue's joint table). */
+typedef struct dd_red_probe {
+  uint32_t warps_per_sm;
+  uint32_t pattern;
+  double adds_per_s;
+} dd_red_probe;
+
+/* Runs the sweep (warps per SM 8, 12, ..., 32 for each pattern, best of three
+ * launches each) and writes up to cap points; *count = points written. */
+int dd_measure_red_sweep(dd_context* ctx, dd_red_probe* out, uint32_t cap, uint32_t* count);
+/* The maximum of that sweep: the device's shared-memory atomic rate, the
+ * bound of the tcgen05 path's histogram epilogue. */
 int dd_measure_red_peak(dd_context* ctx, double* adds_per_s);
 
 /* --- failure detection -------------------------------------------------- */

@@ -30,6 +30,7 @@ def lib() -> C.CDLL:
         L.dd_oracle_an_rows.argtypes = [u64, u32, u64, u64, _u64p, u32]
         L.dd_oracle_an_grid1d.argtypes = [u64, u32, u32, u64, _u64p, u32, _u64p]
         L.dd_oracle_an_grid2d.argtypes = [u64, u32, u64, u64, _u64p, u32]
+        L.dd_oracle_an_grid2d.restype = u64
         L.dd_oracle_an_low_distance.argtypes = [u64, u32, u32, _u64p, _u64p]
         L.dd_oracle_grid1d_points.argtypes = [u64, u32, u32, u64]
         L.dd_oracle_grid1d_points.restype = u64
@@ -129,10 +130,15 @@ def grid2d_points(A: int, n: int, m: int) -> int:
     return lib().dd_oracle_grid2d_points(A, n, m)
 
 
-def an_grid2d_raw(A: int, n: int, m: int, m2: int, nbins: int) -> list[int]:
+def an_grid2d_raw(A: int, n: int, m: int, m2: int, nbins: int, with_bin0: bool = False) -> list[int]:
+    """The reference's raw 2-D grid histogram (bin 0 left at 0), or with
+    with_bin0 the device histogram of every pair (bin 0 = coincident points)."""
     b = _buf()
-    lib().dd_oracle_an_grid2d(A, n, m, m2, b, nbins)
-    return list(b[:nbins])
+    zero = lib().dd_oracle_an_grid2d(A, n, m, m2, b, nbins)
+    out = list(b[:nbins])
+    if with_bin0:
+        out[0] = zero
+    return out
 
 
 def an_grid_counts(gdim: int, n: int, m: int, m2: int, raw: list[int]) -> list[int]:

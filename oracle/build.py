@@ -15,7 +15,9 @@ HERE = Path(__file__).resolve().parent
 OUT = HERE / "_build"
 LIB = OUT / "libdd_oracle.so"
 REF_OUT = HERE / "_ref"
-REF_SRC = Path(os.environ.get("CODREL_REFERENCE", "/root/reference"))
+# The reference checkout: $CODREL_REFERENCE, else a checkout named `reference`
+# beside this repository.
+REF_SRC = Path(os.environ.get("CODREL_REFERENCE", str(HERE.parent.parent / "reference")))
 
 
 def build_oracle() -> Path:

@@ -220,9 +220,12 @@ void dd_oracle_an_grid1d(uint64_t A, unsigned n, unsigned h, uint64_t m, uint64_
 
 /* 2-D grid (dancoding_grid_2d, an_coding_grid.cu:121-140): w_i = A*(T)(i*stepsize2)
  * for i in [0, m2), v_k = A*(T)(k*stepsize) while v_k < A<<n; bin 0 NOT
- * counted.  T is uint32 iff A<<n < 2^32 (an_coding_grid.cu:188). */
-void dd_oracle_an_grid2d(uint64_t A, unsigned n, uint64_t m, uint64_t m2, uint64_t* raw, unsigned nbins)
+ * counted.  T is uint32 iff A<<n < 2^32 (an_coding_grid.cu:188).  Returns the
+ * number of coincident lattice points (the distance-0 pairs the reference's
+ * kernel leaves out of bin 0). */
+uint64_t dd_oracle_an_grid2d(uint64_t A, unsigned n, uint64_t m, uint64_t m2, uint64_t* raw, unsigned nbins)
 {
+  uint64_t zero = 0;
   const uint64_t N = 1ull << n;
   if (m > N) m = N;
   if (m2 > N) m2 = N;
@@ -249,8 +252,12 @@ void dd_oracle_an_grid2d(uint64_t A, unsigned n, uint64_t m, uint64_t m2, uint64
       }
     }
 #pragma omp critical
-    for (unsigned b = 1; b < nbins; ++b) raw[b] += loc[b];
+    {
+      for (unsigned b = 1; b < nbins; ++b) raw[b] += loc[b];
+      zero += loc[0];
+    }
   }
+  return zero;
 }
 
 /* ------------------------------------------------------------------ */

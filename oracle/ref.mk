@@ -7,7 +7,11 @@
 #
 #   make -f oracle/ref.mk REF=/path/to/coding_reliability
 #
-REF      ?= /root/reference
+# REF is required (oracle/build.py passes $CODREL_REFERENCE, or the checkout
+# named `reference` beside this repository).
+ifndef REF
+$(error REF=<reference checkout> is required)
+endif
 OUT      ?= $(dir $(lastword $(MAKEFILE_LIST)))_ref
 NVCC     ?= nvcc
 DD       := $(REF)/distance_distribution

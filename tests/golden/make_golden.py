@@ -1,7 +1,7 @@
 """Generates the golden fixtures under tests/golden/ from the reference.
 
-Sources (all read from the reference checkout, path in CODREL_REFERENCE,
-default /root/reference):
+Sources (all read from the reference checkout: $CODREL_REFERENCE, else the
+checkout named `reference` beside this repository):
   * distance_distribution/src/solutions.h           exact AN / Ext-Hamming tables
   * distance_distribution/results/As/*.csv          exhaustive AN histograms (many A, n=8..24)
   * distance_distribution/results/{GridMs,converge/geom,runtimes/0,As}/*grid1d*.csv
@@ -28,7 +28,9 @@ from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
 ROOT = HERE.parent.parent
-REF = Path(os.environ.get("CODREL_REFERENCE", "/root/reference"))
+# the reference checkout: $CODREL_REFERENCE, else a checkout named `reference`
+# beside this repository
+REF = Path(os.environ.get("CODREL_REFERENCE", str(ROOT.parent / "reference")))
 RES = REF / "distance_distribution" / "results"
 sys.path.insert(0, str(ROOT))
 

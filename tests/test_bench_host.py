@@ -1,0 +1,38 @@
+"""Host-side pieces of bench.py that need no GPU: the serving mix covers every
+query class of the serving configuration (the k=32 grid included), and the
+latency percentiles are nearest-rank."""
+import sys
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent.parent
+sys.path.insert(0, str(ROOT))
+
+import bench  # noqa: E402
+import coding_reliability_b200 as dd  # noqa: E402
+
+
+def test_serving_mix_covers_every_class():
+    mix = bench.serving_mix(dd)
+    assert len(mix) == 48
+    seen = set()
+    for cls, q in mix:
+        assert 129 <= q.A < 1 << 16 and q.A % 2 == 1
+        assert q.n in (8, 12, 16, 20, 24, 32)
+        if q.n <= 20:
+            assert cls == "exhaustive" and q.mode == dd.MODE_EXHAUSTIVE
+        elif cls == "grid":
+            assert q.mode == dd.MODE_GRID_1D and q.m == 1 << 16  # stride 2^(k-16)
+        else:
+            assert cls == "monte_carlo" and q.mode == dd.MODE_MONTE_CARLO
+            assert 1 << 32 <= (q.m << q.n) <= 1 << 36 or q.m == 1
+        seen.add((cls, q.n))
+    assert ("grid", 32) in seen and ("grid", 24) in seen
+    assert {c for c, _ in seen} == set(bench.SERVING_CLASSES)
+
+
+def test_percentile_is_nearest_rank():
+    v = sorted(float(x) for x in range(1, 49))
+    assert bench.percentile(v, 0.50) == 24.0
+    assert bench.percentile(v, 0.99) == 48.0
+    assert bench.percentile([5.0], 0.99) == 5.0
+    assert bench.percentile(sorted(float(x) for x in range(1, 101)), 0.99) == 99.0

@@ -21,30 +21,40 @@ CASES = [
     (dd.Request(dd.CODE_AN, dd.MODE_EXHAUSTIVE, 641, 13, kernel=dd.KERNEL_MMA), "mma"),
     (dd.Request(dd.CODE_AN, dd.MODE_GRID_1D, 58659, 18, m=77, kernel=dd.KERNEL_POPC), "popc"),
     (dd.Request(dd.CODE_AN, dd.MODE_GRID_1D, 58659, 18, m=77, kernel=dd.KERNEL_MMA), "mma"),
+    (dd.Request(dd.CODE_AN, dd.MODE_GRID_2D, 61, 14, m=300, m2=129, kernel=dd.KERNEL_POPC), "popc"),
     (dd.Request(dd.CODE_AN, dd.MODE_GRID_2D, 61, 14, m=300, m2=129, kernel=dd.KERNEL_MMA), "mma"),
-    (dd.Request(dd.CODE_AN, dd.MODE_MONTE_CARLO, 641, 12, m=16, seed=5), "popc"),
+    (dd.Request(dd.CODE_AN, dd.MODE_MONTE_CARLO, 641, 12, m=16, seed=5, kernel=dd.KERNEL_POPC), "popc"),
     # 256 codewords: 8 tiles of which 6 lie past the last row, so some parts hold no strip at all
     (dd.Request(dd.CODE_EXT_HAMMING, dd.MODE_EXHAUSTIVE, 1, 8, with_1bit=1,
                 hamming_method=dd.HAMMING_ALL_PAIRS, kernel=dd.KERNEL_MMA), "mma"),
-    (dd.Request(dd.CODE_EXT_HAMMING, dd.MODE_EXHAUSTIVE, 1, 16, with_1bit=1), "popc"),
+    (dd.Request(dd.CODE_EXT_HAMMING, dd.MODE_EXHAUSTIVE, 1, 16, with_1bit=1, kernel=dd.KERNEL_POPC), "popc"),
 ]
 
 
-@pytest.mark.parametrize("req,kern", CASES, ids=[f"{c[0].code}-{c[0].mode}-{c[0].A}-{c[0].n}-{c[1]}" for c in CASES])
-def test_parts_sum_to_the_whole(ctx, req, kern):
+# the tcgen05 cases run under each epilogue
+VARIANTS = [(q, k, e) for q, k in CASES for e in ((dd.MMA_EPILOGUE_PAIRED, dd.MMA_EPILOGUE_SINGLE)
+                                                   if k == "mma" else (dd.MMA_EPILOGUE_AUTO,))]
+
+
+@pytest.mark.parametrize("req,kern,epi", VARIANTS,
+                         ids=[f"{c[0].code}-{c[0].mode}-{c[0].A}-{c[0].n}-{c[1]}{c[2] or ''}" for c in VARIANTS])
+def test_parts_sum_to_the_whole(ctx, req, kern, epi):
+    ctx.set_mma_epilogue(epi)
     full = ctx.histogram(req)
+    assert full.kernel_used == (dd.KERNEL_MMA if kern == "mma" else dd.KERNEL_POPC)
     if kern == "mma":
-        assert full.kernel_used == dd.KERNEL_MMA
+        assert full.mma_epilogue == epi
     total = dd.request_plan(req)["tiles"]
     raw = None
     for b, e in reversed(bounds(total)):  # any order
         raw, _ = ctx.histogram_part(req, b, e - b, raw)
     assert raw == full.raw[:full.nbins]
     assert dd.postprocess(req, raw).counts == full.counts
+    ctx.set_mma_epilogue(dd.MMA_EPILOGUE_AUTO)
 
 
-def test_resumable_equals_one_call(ctx, tmp_path):
-    req = dd.Request(dd.CODE_AN, dd.MODE_EXHAUSTIVE, 58659, 18)
+def test_resumable_equals_one_call(ctx, kernel, tmp_path):
+    req = dd.Request(dd.CODE_AN, dd.MODE_EXHAUSTIVE, 58659, 18, kernel=int(kernel))
     res = dd.run_resumable(ctx, req, tmp_path / "k18.json", chunk_tiles=1001)
     assert res.counts == ctx.histogram(req).counts
 

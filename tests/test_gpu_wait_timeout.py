@@ -10,11 +10,16 @@ import coding_reliability_b200 as dd
 pytestmark = pytest.mark.gpu
 
 
-def test_wait_timeout_is_reported_and_the_context_recovers():
+@pytest.mark.parametrize("epilogue", ["paired", "single"])
+def test_wait_timeout_is_reported_and_the_context_recovers(epilogue):
+    """Both tcgen05 epilogues: the paired one also waits at its epilogue-wide
+    barriers around the table flushes, which give up the same way."""
     q = dd.Request(dd.CODE_AN, dd.MODE_EXHAUSTIVE, 58659, 18, kernel=dd.KERNEL_MMA)
     with dd.Context(0) as ctx:
+        e = dd.MMA_EPILOGUE_PAIRED if epilogue == "paired" else dd.MMA_EPILOGUE_SINGLE
+        ctx.set_mma_epilogue(e)
         good = ctx.histogram(q)
-        assert good.kernel_used == dd.KERNEL_MMA
+        assert good.kernel_used == dd.KERNEL_MMA and good.mma_epilogue == e
         ctx.set_wait_timeout(1)
         for _ in range(2):
             with pytest.raises(dd.DDError) as e:

@@ -90,7 +90,9 @@ GPU_CASES = [c for c in CONV if compared(c) and (c["n"] == 16 or c["m"] <= 101)]
 def test_gpu_mc_agrees_with_reference_runs(ctx, case):
     import coding_reliability_b200 as dd
     n, m = case["n"], case["m"]
-    res = ctx.histogram(dd.Request(dd.CODE_AN, dd.MODE_MONTE_CARLO, 61, n, m=m, seed=2000 + m))
+    res = ctx.histogram(dd.Request(dd.CODE_AN, dd.MODE_MONTE_CARLO, 61, n, m=m, seed=2000 + m,
+                                   kernel=dd.KERNEL_POPC))
+    assert res.kernel_used == dd.KERNEL_POPC  # Monte Carlo runs on the popc kernel
     X = sample_counts(res.counts, n, m)
     # 6 standard errors (the same seeds replayed by the oracle's Philox pass these bounds)
     check_against_exact(X, n, m, z=6.0)

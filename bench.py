@@ -58,6 +58,10 @@ def parse():
     p.add_argument("--impl", default="b200", choices=["b200", "reference"])
     p.add_argument("--workload", default="an_k24", choices=["an_k24", "an_k20", "an_k22"])
     p.add_argument("--kernel", default="auto", choices=["auto", "popc", "mma"])
+    p.add_argument("--epilogue", default="auto", choices=["auto", "paired", "single"],
+                   help="tcgen05 epilogue (auto: the autotuner's choice); pin it where a profiler's overhead "
+                        "could change the autotuner's choice")
+    p.add_argument("--launch-log", default="", help="write every launch's CUDA-event time (JSON) to this file")
     p.add_argument("--no-extras", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-parity", action="store_true", help="skip the cross-kernel check of the headline histogram")
@@ -248,6 +252,14 @@ def main() -> None:
     A, k = WORKLOADS[args.workload]
     kernel = {"auto": dd.KERNEL_AUTO, "popc": dd.KERNEL_POPC, "mma": dd.KERNEL_MMA}[args.kernel]
     tuning = ctx.autotune() if kernel == dd.KERNEL_AUTO else None
+    if args.epilogue != "auto":
+        ctx.set_mma_epilogue(dd.MMA_EPILOGUE_PAIRED if args.epilogue == "paired" else dd.MMA_EPILOGUE_SINGLE)
+    launches = []  # (phase, kernel, ms): CUDA-event times, for --launch-log
+    if tuning:
+        for name, key in (("popc_red", "popc_red_pairs_per_s"), ("popc_ldst", "popc_ldst_pairs_per_s"),
+                          ("mma_single", "mma_single_pairs_per_s"), ("mma_paired", "mma_paired_pairs_per_s")):
+            launches.append(("autotune probe A=65521 k=20 (best of 2 timed, 3 run)", name,
+                             tuning["probe_pairs"] / tuning[key] * 1e3))
     req = dd.Request(dd.CODE_AN, dd.MODE_EXHAUSTIVE, A, k, kernel=kernel)
     P = pairs_of(k)
 
@@ -258,8 +270,12 @@ def main() -> None:
             dist.barrier()
         torch.cuda.synchronize()
 
+    def kname(r):
+        return ("mma_" + dd.EPILOGUE_NAMES.get(r.mma_epilogue, "?")) if r.kernel_used == dd.KERNEL_MMA else "popc"
+
     for _ in range(args.warmup):
-        ctx.histogram(req)
+        r = ctx.histogram(req)
+        launches.append((f"warm-up A={A} k={k}", kname(r), r.kernel_ms))
     popc_peak = ctx.popc_peak()  # popc/s, measured on this GPU now
     red_sweep = ctx.red_sweep()  # shared-memory atomic adds/s at 8..32 warps per SM, both table layouts
     red_best = max(red_sweep, key=lambda r: r["adds_per_s"])
@@ -275,6 +291,8 @@ def main() -> None:
         r = ctx.histogram(req)
         kernel_ms += r.kernel_ms
         results.append(r)
+    for r in results:
+        launches.append((f"timed A={A} k={k}", kname(r), r.kernel_ms))
     ev1.record(stream)
     barrier()
     total_ms = ev0.elapsed_time(ev1)
@@ -289,6 +307,7 @@ def main() -> None:
     parity = None
     if rank == 0 and not args.no_parity:
         parity = cross_kernel_check(ctx, dd, A, k, results[0])
+        launches.append((f"parity A={A} k={k}", parity["other_kernel"], pairs_of(k) / parity["other_kernel_pairs_per_s"] * 1e3))
 
     value = replica_throughput(P * args.steps, world, t_kernel)
     e2e = replica_throughput(P * args.steps, world, t_total)
@@ -315,6 +334,8 @@ def main() -> None:
                                    "per SM and two table layouts (dd_measure_red_sweep); best at "
                                    f"{red_best['warps_per_sm']} warps, {red_best['pattern']}",
                     "peak_by_layout_gred_s": {k: v / 1e9 for k, v in per_pattern.items()},
+                    "peak_sweep_gred_s": [[r["warps_per_sm"], r["pattern"], round(r["adds_per_s"] / 1e9, 1)]
+                                          for r in red_sweep],
                     "popc_path_equivalent_frac": per_gpu / popc_peak,
                     # the tensor pipe beside it: 2 * K int8 operations per MMA column
                     "tensor_pipe": {"achieved_tops": per_gpu * 2 * k_per_pair / 1e12,
@@ -355,6 +376,10 @@ def main() -> None:
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
+    if rank == 0 and args.launch_log:
+        Path(args.launch_log).write_text(json.dumps(
+            {"command": " ".join(sys.argv), "launches": [{"phase": a, "kernel": b, "ms": c} for a, b, c in launches]},
+            indent=1))
     if rank == 0:
         print(json.dumps(line), flush=True)
 

@@ -132,21 +132,29 @@ __host__ __device__ __forceinline__ uint64_t lattice_value(uint64_t A, uint64_t 
 }
 
 // Upper-triangle decode (both kernels' super-tile order): s in [0, M(M+1)/2)
-// -> (r, c), r <= c, row-major.  The square root only seeds the row; the two
-// loops correct it exactly against the integer row starts.
+// -> (r, c), r <= c, column by column: column c holds rows 0..c, and
+// T(c) = c(c+1)/2 entries precede it.  Consecutive super tiles share their
+// columns, so the tcgen05 kernel keeps one column operand for a run of them.
+// The square root only seeds the column; the two loops correct it exactly
+// against the integer column starts.
 __device__ __forceinline__ void tri_decode(uint64_t s, uint64_t M, uint64_t& r, uint64_t& c) {
-  const double b = 2.0 * (double)M + 1.0;
-  double disc = b * b - 8.0 * (double)s;
-  if (disc < 0) disc = 0;
-  int64_t rr = (int64_t)((b - sqrt(disc)) * 0.5);
-  if (rr < 0) rr = 0;
-  if ((uint64_t)rr >= M) rr = (int64_t)M - 1;
-  auto S = [M](uint64_t r_) { return r_ * M - (r_ * (r_ - (r_ ? 1 : 0))) / 2; };
-  // S(r) = r*M - r*(r-1)/2 entries precede row r
-  while ((uint64_t)rr + 1 < M && S((uint64_t)rr + 1) <= s) ++rr;
-  while (rr > 0 && S((uint64_t)rr) > s) --rr;
-  r = (uint64_t)rr;
-  c = r + (s - S(r));
+  double x = (sqrt(8.0 * (double)s + 1.0) - 1.0) * 0.5;
+  int64_t cc = (int64_t)x;
+  if (cc < 0) cc = 0;
+  if ((uint64_t)cc >= M) cc = (int64_t)M - 1;
+  auto T = [](uint64_t c_) { return c_ * (c_ + 1) / 2; };
+  while ((uint64_t)cc + 1 < M && T((uint64_t)cc + 1) <= s) ++cc;
+  while (cc > 0 && T((uint64_t)cc) > s) --cc;
+  c = (uint64_t)cc;
+  r = s - T(c);
+}
+
+// Tile lt of a grid (rectangle) job: 128 rows x 1024 columns, column tile by
+// column tile (both kernels), so consecutive tiles share their columns.
+// row_tiles = ceil(rows / 128).
+__host__ __device__ __forceinline__ void rect_decode(uint64_t lt, uint64_t row_tiles, uint64_t& r0, uint64_t& c0) {
+  r0 = (lt % row_tiles) * 128;
+  c0 = (lt / row_tiles) * 1024;
 }
 
 }  // namespace dd

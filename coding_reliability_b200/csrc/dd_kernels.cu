@@ -187,9 +187,8 @@ __device__ void pairs_tile(const Job& J, uint64_t lt, uint32_t* wbins, uint32_t*
     c1 = c0 + kSuper < J.cols ? c0 + kSuper : J.cols;
     diag = (sr == sc);
   } else {
-    const uint64_t rt = lt / J.col_tiles, ct = lt % J.col_tiles;
-    r0 = rt * kWarpRows;
-    c0 = ct * kTileCols;
+    static_assert(kWarpRows == 128 && kTileCols == 1024, "rect_decode's tile shape");
+    rect_decode(lt, (J.rows + kWarpRows - 1) / kWarpRows, r0, c0);
     c1 = c0 + kTileCols < J.cols ? c0 + kTileCols : J.cols;
   }
   if (r0 >= J.rows) return;
@@ -556,14 +555,16 @@ __global__ void __launch_bounds__(256) popc_rate_kernel(uint32_t iters, uint32_t
 
 // Shared-memory atomic rate, measured the way the tcgen05 kernel's epilogues
 // use the pipe: one CTA per SM of blockDim.x threads, every thread adding 1 in
-// a 128 KB table, 32 independent adds per loop iteration, conflict-free within
+// a 128 KB table, 32 independent adds per loop iteration to addresses held in
+// registers (so no address arithmetic limits the rate), conflict-free within
 // each warp (the 32 lanes always hit 32 banks).
 //   kRedPerThread: every thread its own column of 32 rows (row stride
-//                  blockDim.x words), the row changing with every add (the
-//                  single epilogue's per-thread bins);
+//                  blockDim.x words), a different row for each of its 32 adds
+//                  (the single epilogue's per-thread bins);
 //   kRedLaneShared: one column per lane shared by every warp of the CTA, 1024
-//                  cells, the cell changing with every add and differing
-//                  between warps (the paired epilogue's joint table).
+//                  cells, 32 cells per thread spread like distances around the
+//                  middle of the table and differing between warps (the paired
+//                  epilogue's joint table).
 constexpr int kRedRows = 32;
 constexpr uint32_t kRedCells = 1024;
 enum RedPattern : int { kRedPerThread = 0, kRedLaneShared = 1 };
@@ -571,22 +572,29 @@ enum RedPattern : int { kRedPerThread = 0, kRedLaneShared = 1 };
 template <int kPattern>
 __global__ void __launch_bounds__(1024, 1) red_rate_kernel(uint32_t iters, uint32_t* sink) {
   extern __shared__ uint32_t tab[];
-  const uint32_t nthr = blockDim.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const uint32_t nthr = blockDim.x, tid = threadIdx.x, lane = tid & 31;
   const uint32_t words = kPattern == kRedPerThread ? kRedRows * nthr : kRedCells * 32u;
   for (uint32_t k = tid; k < words; k += nthr) tab[k] = 0;
   __syncthreads();
   const uint32_t sbase = (uint32_t)__cvta_generic_to_shared(tab);
+  uint32_t a[32];
+#pragma unroll
+  for (uint32_t u = 0; u < 32; ++u) {
+    if constexpr (kPattern == kRedPerThread) {
+      a[u] = sbase + tid * 4u + ((u * 7u) & (kRedRows - 1)) * nthr * 4u;
+    } else {
+      // two 16-bit popcounts of a hash: a binomial-like cell around 512
+      uint32_t h = (tid * 32u + u) * 0x9E3779B1u;
+      h ^= h >> 15;
+      h *= 0x85EBCA77u;
+      h ^= h >> 13;
+      const uint32_t cell = (__popc(h & 0xFFFFu) + __popc(h >> 16)) * 31u;  // [0, 32 * 31] < kRedCells
+      a[u] = sbase + lane * 4u + cell * 128u;
+    }
+  }
   for (uint32_t i = 0; i < iters; ++i) {
 #pragma unroll
-    for (uint32_t u = 0; u < 32; ++u) {
-      uint32_t a;
-      if constexpr (kPattern == kRedPerThread) {
-        a = sbase + tid * 4u + (((i + u * 7u) & (kRedRows - 1)) * nthr) * 4u;
-      } else {
-        a = sbase + lane * 4u + (((i * 32u + u) * 37u + warp * 101u) & (kRedCells - 1)) * 128u;
-      }
-      asm volatile("red.shared.add.u32 [%0], 1;" ::"r"(a) : "memory");
-    }
+    for (uint32_t u = 0; u < 32; ++u) asm volatile("red.shared.add.u32 [%0], 1;" ::"r"(a[u]) : "memory");
   }
   __syncthreads();
   uint32_t s = 0;

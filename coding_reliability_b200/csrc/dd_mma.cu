@@ -28,19 +28,21 @@
 // tensor-memory loads and column-operand bytes per pair.
 //
 // Work unit: the popc kernel's tile space (1024x1024 super tiles of the i<j
-// triangle, split into 8 strips of 128 rows; for grid jobs, 128 lattice rows x
-// 1024 columns, taken column-major).  A strip is 128 rows (UMMA M) x
+// triangle, column by column, split into 8 strips of 128 rows; for grid jobs,
+// 128 lattice rows x 1024 columns, column tile by column tile; tri_decode and
+// rect_decode in dd_device.cuh).  A strip is 128 rows (UMMA M) x
 // 1024 columns = 4 MMA tiles of N = 256 (single) or 2 tiles of N = 256 packed
 // columns, accumulated in two TMEM buffers of 256 columns: the MMA of tile t+1
 // runs while the epilogue bins tile t.  (Four buffers of N = 128 measured 17 %
 // slower for the single epilogue: every tile costs each epilogue warp a barrier
 // poll and an arrive through the shared-memory pipe that its atomics saturate,
-// so fewer, wider tiles win over deeper buffering.)  Generator warps claim 8
-// strips at a time (one super tile when the job's tile range is aligned) and
-// write the column operand once per super tile, into the second of two
-// buffers when both fit beside the bins, so the next super tile's operand is
-// written while the current one's MMAs run; the row operand is double-buffered
-// by strip.  One CTA per SM (16 epilogue warps, 1 issuer warp, 3 generator
+// so fewer, wider tiles win over deeper buffering.)  Generator warps claim 32
+// strips at a time (four super tiles when the job's tile range is aligned,
+// which in the column-by-column order mostly share one column) and write the
+// column operand only when the column super tile changes, into the second of
+// two buffers when both fit beside the bins, so the next operand is written
+// while the current one's MMAs run; the row operand is double-buffered by
+// strip.  One CTA per SM (16 epilogue warps, 1 issuer warp, 3 generator
 // warps, 512 TMEM columns).
 //
 // The single epilogue is bound by the shared-memory atomic rate (one
@@ -98,6 +100,9 @@ constexpr unsigned kGenPollNs = 0;
 constexpr int kColsPerWarp = kN / (kEpiWarps / 4);  // columns of a tile each epilogue warp reads
 constexpr int kLoads = kColsPerWarp / 32;           // 32-column TMEM loads per warp and tile
 static_assert(kEpiWarps % 4 == 0 && kColsPerWarp % 32 == 0, "whole 32-column TMEM loads per warp and tile");
+// Strips a generator claim takes: 4 super tiles, which in the column-by-column
+// tile order share their column operand (written once per claim and column).
+constexpr int kClaimStrips = 4 * kStrips;
 // pair-packed epilogue
 constexpr int kPkHalf = kSuper / 2;                 // column p of a strip pairs with column p + 512
 constexpr int kPkTilesPerStrip = kPkHalf / kN;      // 2 MMA tiles of 256 packed columns per strip
@@ -310,10 +315,11 @@ __device__ __forceinline__ uint64_t mma_col_value(const Job* J, uint64_t j) {
 struct Shared {
   uint64_t full[kBufs];   // tile in TMEM buffer b ready: tcgen05.commit + the issuer's arrive (count 2)
   uint64_t empty[kBufs];  // TMEM buffer b read: one arrive per epilogue warp (count kEpiWarps)
-  // strip info for the epilogue, by issued strip (tile g belongs to strip g / kTilesPerStrip):
-  // read once per strip, so the epilogue's per-tile shared-memory traffic is the
-  // barrier poll and arrive only (its loads would queue behind the atomics)
-  StripInfo estrip[2];
+  // strip info for the epilogue, by issued strip (tile g belongs to strip g / tiles
+  // per strip), a ring of 4: read once per strip, so the epilogue's per-tile
+  // shared-memory traffic is the barrier poll and arrive only (its loads would
+  // queue behind the atomics)
+  StripInfo estrip[4];
   // strip queue, generators -> issuer (slot = strip & 1, with that slot's row operand)
   StripInfo strip[2];
   uint64_t slot_full[2];  // strip ready: the generators' thread 0 arrives (count 1)
@@ -382,10 +388,16 @@ __device__ __forceinline__ bool epi_sync(Shared* sh, uint32_t& phase, int lane, 
 
 // Two single distances of a packed value (fallback row), for the outliers of
 // full tiles and the checked pairs of partial tiles: Q = P + S*lo = d1 + S*d2.
-__device__ __forceinline__ void pk_decode(uint32_t P, uint32_t S, int32_t lo, uint32_t& d1, uint32_t& d2) {
+// False for a value no operands can produce (d2 >= kPkFb).  Q < 64 * S <= 3904
+// is exact in float, and (Q + 1/2) / S lies at least 1/(2S) from an integer,
+// far above the error of the rounded reciprocal.
+__device__ __forceinline__ bool pk_decode(uint32_t P, uint32_t S, float inv_s, int32_t lo, uint32_t& d1,
+                                          uint32_t& d2) {
   const uint32_t Q = P + S * (uint32_t)lo;
-  d2 = Q / S;
+  if (Q >= S * kPkFb) return false;
+  d2 = (uint32_t)(((float)Q + 0.5f) * inv_s);
   d1 = Q - d2 * S;
+  return true;
 }
 
 // Warp roles: warps 0..15 bin (epilogue), warp 16 issues the MMAs (lane 0),
@@ -458,14 +470,14 @@ __global__ void __launch_bounds__(kThreads, 1) mma_hist_kernel(MmaArgs args) {
     bool normal = false;
     for (;;) {
       if (t >= end) {
-        if (gtid == 0) sh->gclaim[nclaim & 1] = atomicAdd(args.counter, (unsigned long long)kStrips);
+        if (gtid == 0) sh->gclaim[nclaim & 1] = atomicAdd(args.counter, (unsigned long long)kClaimStrips);
         gen_bar();
         const unsigned long long base = sh->gclaim[nclaim & 1];
         ++nclaim;
         if (base >= args.total_tiles) { normal = true; break; }
         t = base;
-        end = base + kStrips < args.total_tiles ? base + (unsigned long long)kStrips
-                                                : (unsigned long long)args.total_tiles;
+        end = base + kClaimStrips < args.total_tiles ? base + (unsigned long long)kClaimStrips
+                                                     : (unsigned long long)args.total_tiles;
       }
       const unsigned long long tt = t++;
       const uint32_t jn = find_job(args.jobs, args.njobs, tt);
@@ -485,12 +497,11 @@ __global__ void __launch_bounds__(kThreads, 1) mma_hist_kernel(MmaArgs args) {
       uint64_t r0, c0, sc;
       bool full;
       if (rect) {
-        // grid job: 128 rows x 1024 columns per tile, column-major here so that
-        // consecutive tiles share the column operand
-        const uint64_t row_tiles = (N + kM - 1) / kM;
-        sc = lt / row_tiles;
-        r0 = (lt % row_tiles) * kM;
-        c0 = sc * kSuper;
+        // grid job: 128 rows x 1024 columns per tile, column tile by column tile,
+        // so that consecutive tiles share the column operand
+        static_assert(kM == 128 && kSuper == 1024, "rect_decode's tile shape");
+        rect_decode(lt, (N + kM - 1) / kM, r0, c0);
+        sc = c0 / kSuper;
         full = (r0 + kM <= N) && (c0 + kSuper <= NC);
       } else {
         uint64_t sr;
@@ -606,9 +617,9 @@ __global__ void __launch_bounds__(kThreads, 1) mma_hist_kernel(MmaArgs args) {
           if (!wait_empty(g)) { ok = false; break; }
           const uint32_t b = buf_of(g);
           if (tile == 0) {
-            // the entry of strip s-2: every warp read it at tile g-2*kTps, before
-            // tile g-kBufs, which wait_empty has seen read
-            StripInfo& es = sh->estrip[(g / kTps) & 1];
+            // the entry of strip s-4: every warp read it at tile g-4*kTps, long
+            // before tile g-kBufs, which wait_empty has seen released
+            StripInfo& es = sh->estrip[(g / kTps) & 3];
             es = si;
             es.flags = si.flags & (kInfoFull | kInfoRect);
           }
@@ -626,7 +637,7 @@ __global__ void __launch_bounds__(kThreads, 1) mma_hist_kernel(MmaArgs args) {
       }
       if (normal && wait_empty(g)) {
         // end of work: a strip marked done wakes the epilogue warps (g is a strip's first tile)
-        sh->estrip[(g / kTps) & 1].flags = kInfoDone;
+        sh->estrip[(g / kTps) & 3].flags = kInfoDone;
         mbar_arrive(smem_u32(&sh->full[buf_of(g)]));
         mbar_arrive(smem_u32(&sh->full[buf_of(g)]));
       } else {
@@ -648,6 +659,8 @@ __global__ void __launch_bounds__(kThreads, 1) mma_hist_kernel(MmaArgs args) {
     const uint32_t pk_fb = pk_lane + (args.pk_cells << 7);
     uint32_t pkS = 1, pklimit = 0, epi_phase = 0;
     int32_t pklo = 0;
+    float pkinv = 1.0f;
+    bool pkall = false;  // the window holds every (d1, d2): no value can fall outside it
     // single: this warp's bin columns -> the job's global bins
     auto flush = [&]() {
       for (uint32_t b = 0; b < args.hist_rows; ++b) {
@@ -698,8 +711,7 @@ __global__ void __launch_bounds__(kThreads, 1) mma_hist_kernel(MmaArgs args) {
     // pair-packed: one packed value counted as two single distances (fallback row)
     auto pk_single = [&](uint32_t P, bool v1, bool v2) {
       uint32_t d1, d2;
-      pk_decode(P, pkS, pklo, d1, d2);
-      if (d2 >= kPkFb) {  // not a value the operands can produce
+      if (!pk_decode(P, pkS, pkinv, pklo, d1, d2)) {  // not a value the operands can produce
         atomicOr(args.status, KSTATUS_BAD_DISTANCE);
         return;
       }
@@ -708,59 +720,58 @@ __global__ void __launch_bounds__(kThreads, 1) mma_hist_kernel(MmaArgs args) {
     };
     unsigned long long r0 = 0, cs = 0, n = 0, nc = 0;  // the current strip: first row and column, rows, columns
     uint32_t flags = 0, job = 0;
-    for (uint64_t g = 0;; ++g) {
-      const uint32_t b = buf_of(g);
+    // lane 0 waits (bounded) for tile g; the warp learns the result
+    auto wait_full = [&](uint64_t g) -> bool {
       bool r = true;
-      if (lane == 0) r = wait_or_abort<kEpiPollNs>(smem_u32(&sh->full[b]), parity_of(g), args.timeout_ns, abort);
-      if (!__shfl_sync(0xffffffffu, r ? 1 : 0, 0)) { ok = false; break; }
+      if (lane == 0) r = wait_or_abort<kEpiPollNs>(smem_u32(&sh->full[buf_of(g)]), parity_of(g), args.timeout_ns, abort);
+      const bool ok_ = __shfl_sync(0xffffffffu, r ? 1 : 0, 0) != 0;
       __syncwarp();  // lane 0's wait acquired the MMA result (and StripInfo); this orders it for the warp
-      const uint32_t tile = (uint32_t)(g % kTps);
-      if (tile == 0) {
-        const StripInfo& es = sh->estrip[(g / kTps) & 1];
-        flags = es.flags;
-        if (flags & kInfoDone) break;
-        job = es.job;
+      return ok_;
+    };
+    // the strip that tile g (a strip's first tile) starts; false at the end marker
+    auto read_strip = [&](uint64_t g) -> bool {
+      const StripInfo& es = sh->estrip[(g / kTps) & 3];
+      flags = es.flags;
+      if (flags & kInfoDone) return false;
+      job = es.job;
+      if constexpr (!kPk) {  // the paired epilogue reads them from es where it needs them
         r0 = es.r0;
         cs = es.c0;
         n = es.n;
         nc = es.cols;
       }
-      if constexpr (kPk) {
-        // a new job: the table must hold one job's counts, so every warp folds it
-        // first (all warps see the same strips, so they flush at the same tile)
-        if (job != cur) {
-          if (cur != 0xffffffffu && !flush_pk()) { ok = false; break; }
-          since_flush = 0;
-          cur = job;
-          bins = args.jobs[job].bins;
-          nbins = args.jobs[job].nbins;
-          pkS = args.jobs[job].pk_s;
-          pklo = args.jobs[job].pk_lo;
-          pklimit = args.jobs[job].pk_limit;  // <= pk_cells (host)
-        }
-      }
-      tc_fence_after();
-      uint32_t v[kLoads][32];
+      return true;
+    };
+    // 32 TMEM columns (half h of this warp's 64) of tile g: issued, completed by tmem_wait_ld
+    auto ld_half = [&](uint64_t g, int h, uint32_t (&dst)[32]) {
+      tmem_ld32_nowait(tmem + ((uint32_t)(q * 32) << 16) + buf_of(g) * (uint32_t)kN +
+                           (uint32_t)(sub * kColsPerWarp + 32 * h),
+                       dst);
+    };
+    if constexpr (kPk) {
+      auto set_job = [&](uint32_t jb) {
+        cur = jb;
+        bins = args.jobs[jb].bins;
+        nbins = args.jobs[jb].nbins;
+        pkS = args.jobs[jb].pk_s;
+        pklo = args.jobs[jb].pk_lo;
+        pklimit = args.jobs[jb].pk_limit;  // <= pk_cells (host)
+        pkinv = 1.0f / (float)pkS;
+        // lo = 0 and S rows: every value d1 + S*d2 < S*S = limit, the test is void
+        pkall = pklo == 0 && pklimit == pkS * pkS;
+      };
+      // bins 32 packed values, half h of tile g of the current strip
+      auto bin_half = [&](const uint32_t (&x)[32], uint64_t g, int h) {
+        if ((flags & kInfoFull) && pkall) {
 #pragma unroll
-      for (int h = 0; h < kLoads; ++h)
-        tmem_ld32_nowait(tmem + ((uint32_t)(q * 32) << 16) + b * (uint32_t)kN + (uint32_t)(sub * kColsPerWarp + 32 * h),
-                         v[h]);
-      tmem_wait_ld();
-      // the buffer may be refilled as soon as every warp has its values in registers
-      tc_fence_before();
-      __syncwarp();
-      if (lane == 0) mbar_arrive(smem_u32(&sh->empty[b]));
-      if constexpr (kPk) {
-        if (flags & kInfoFull) {
-          // one unsigned max over the tile's values tests every d2 against the
-          // window at once (a d2 below it gives a negative value, i.e. a huge
-          // one); taken as a tree of depth 6, not a chain of 64 dependent maxima:
-          // every epilogue warp reaches this point at the same time
-          static_assert(kLoads == 2, "the max tree takes two 32-value loads");
+          for (int u = 0; u < 32; ++u) red_shared(pk_lane + (x[u] << 7));
+        } else if (flags & kInfoFull) {
+          // one unsigned max over the values tests every d2 against the window
+          // at once (a d2 below it gives a negative value, i.e. a huge one);
+          // a tree of depth 5, not a chain of dependent maxima
           uint32_t m[16];
 #pragma unroll
-          for (int u = 0; u < 16; ++u)
-            m[u] = max(max(v[0][2 * u], v[0][2 * u + 1]), max(v[1][2 * u], v[1][2 * u + 1]));
+          for (int u = 0; u < 16; ++u) m[u] = max(x[2 * u], x[2 * u + 1]);
 #pragma unroll
           for (int w = 8; w >= 1; w >>= 1)
 #pragma unroll
@@ -768,39 +779,78 @@ __global__ void __launch_bounds__(kThreads, 1) mma_hist_kernel(MmaArgs args) {
           if (__any_sync(0xffffffffu, m[0] >= pklimit)) {
             // some d2 outside the window: those values count as two single distances
 #pragma unroll
-            for (int h = 0; h < kLoads; ++h)
-#pragma unroll
-              for (int u = 0; u < 32; ++u) {
-                if (v[h][u] < pklimit) red_shared(pk_lane + (v[h][u] << 7));
-                else pk_single(v[h][u], true, true);
-              }
+            for (int u = 0; u < 32; ++u) {
+              if (x[u] < pklimit) red_shared(pk_lane + (x[u] << 7));
+              else pk_single(x[u], true, true);
+            }
           } else {
 #pragma unroll
-            for (int h = 0; h < kLoads; ++h)
-#pragma unroll
-              for (int u = 0; u < 32; ++u) red_shared(pk_lane + (v[h][u] << 7));
+            for (int u = 0; u < 32; ++u) red_shared(pk_lane + (x[u] << 7));
           }
         } else {
-          // partial strip: every pair checked, counted singly
-          const uint64_t i = r0 + (uint64_t)(q * 32 + lane);
-          const uint64_t j0 = cs + (uint64_t)tile * kN + (uint64_t)(sub * kColsPerWarp);
-          // fully unrolled: the values stay in registers (a loop index into v[][]
-          // would move the array to local memory)
+          // partial strip: every pair checked; a value whose two pairs both count
+          // and whose d2 lies in the window still takes one joint cell.  The
+          // strip's entry stays valid while its tiles are binned: the issuer
+          // rewrites it for strip s+4 only after every warp has released the
+          // tiles of strip s+3.
+          const StripInfo& es = sh->estrip[(g / kTps) & 3];
+          const uint64_t n_ = es.n, nc_ = es.cols;
+          const uint64_t i = es.r0 + (uint64_t)(q * 32 + lane);
+          const uint64_t j0 = es.c0 + (g % kTps) * (uint64_t)kN + (uint64_t)(sub * kColsPerWarp + 32 * h);
 #pragma unroll
-          for (int h = 0; h < kLoads; ++h)
-#pragma unroll
-            for (int u = 0; u < 32; ++u) {
-              const uint64_t j = j0 + 32 * h + u, j2 = j + kPkHalf;
-              const bool v1 = (flags & kInfoRect) ? (i < n && j < nc) : (i < n && j < n && j > i);
-              const bool v2 = (flags & kInfoRect) ? (i < n && j2 < nc) : (i < n && j2 < n && j2 > i);
-              if (v1 || v2) pk_single(v[h][u], v1, v2);
-            }
+          for (int u = 0; u < 32; ++u) {
+            const uint64_t j = j0 + u, j2 = j + kPkHalf;
+            const bool v1 = (flags & kInfoRect) ? (i < n_ && j < nc_) : (i < n_ && j < n_ && j > i);
+            const bool v2 = (flags & kInfoRect) ? (i < n_ && j2 < nc_) : (i < n_ && j2 < n_ && j2 > i);
+            if (v1 && v2 && x[u] < pklimit) red_shared(pk_lane + (x[u] << 7));
+            else if (v1 || v2) pk_single(x[u], v1, v2);
+          }
         }
+      };
+      for (uint64_t g = 0;; ++g) {
+        if (!wait_full(g)) { ok = false; break; }
+        if (g % kTps == 0) {
+          if (!read_strip(g)) break;  // the end marker
+          // a new job: the table must hold one job's counts, so every warp folds
+          // it first (all warps see the same strips, so they flush at the same tile)
+          if (job != cur) {
+            if (cur != 0xffffffffu && !flush_pk()) { ok = false; break; }
+            since_flush = 0;
+            set_job(job);
+          }
+        }
+        tc_fence_after();
+        uint32_t v[kLoads][32];
+#pragma unroll
+        for (int h = 0; h < kLoads; ++h) ld_half(g, h, v[h]);
+        tmem_wait_ld();
+        // the buffer may be refilled as soon as every warp has its values in registers
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(smem_u32(&sh->empty[buf_of(g)]));
+#pragma unroll
+        for (int h = 0; h < kLoads; ++h) bin_half(v[h], g, h);
         if (++since_flush >= kPkFlushTiles) {
           if (!flush_pk()) { ok = false; break; }
           since_flush = 0;
         }
-      } else {
+      }
+      if (ok && cur != 0xffffffffu) flush_pk();
+    } else {
+      for (uint64_t g = 0;; ++g) {
+        const uint32_t b = buf_of(g);
+        if (!wait_full(g)) { ok = false; break; }
+        const uint32_t tile = (uint32_t)(g % kTps);
+        if (tile == 0 && !read_strip(g)) break;
+        tc_fence_after();
+        uint32_t v[kLoads][32];
+#pragma unroll
+        for (int h = 0; h < kLoads; ++h) ld_half(g, h, v[h]);
+        tmem_wait_ld();
+        // the buffer may be refilled as soon as every warp has its values in registers
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(smem_u32(&sh->empty[b]));
         if (job != cur) {
           if (cur != 0xffffffffu && since_flush) flush();
           since_flush = 0;
@@ -829,10 +879,6 @@ __global__ void __launch_bounds__(kThreads, 1) mma_hist_kernel(MmaArgs args) {
         }
         if (++since_flush >= kFlushEvery) { flush(); since_flush = 0; }
       }
-    }
-    if constexpr (kPk) {
-      if (ok && cur != 0xffffffffu) flush_pk();
-    } else {
       if (ok && cur != 0xffffffffu && since_flush) flush();
     }
   }

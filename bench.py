@@ -43,8 +43,11 @@ sys.path.insert(0, str(ROOT))
 
 METRIC = "exact pairs/s (AN k=24 exhaustive histogram)"
 NCU_DRAM_BYTES_PER_LAUNCH = 108288  # popc path: DRAM bytes of one launch, ncu capture at k=20
-NCU_DRAM_BYTES_PER_LAUNCH_MMA = 81408  # tcgen05 path: DRAM bytes of one launch, ncu capture at k=20
-NCU_TENSOR_PIPE_PCT_MMA = 16.9  # sm__pipe_tensor_cycles_active of the same capture
+# tcgen05 path, by epilogue: DRAM bytes of one launch and sm__pipe_tensor_cycles_active
+# of an ncu capture at k=20 (cold caches: the bytes are the job table, the bins and the
+# kernel's own code; codewords are generated on chip)
+NCU_DRAM_BYTES_PER_LAUNCH_MMA = {"paired": 206848, "single": 81408}
+NCU_TENSOR_PIPE_PCT_MMA = {"paired": 11.5, "single": 16.9}
 INT8_DENSE_TOPS_NOMINAL = 4500.0  # B200 dense int8 tensor rate (nominal; the measured peaks cover bf16 only)
 MMA_K_PAD = 64  # int8 K of every tcgen05 tile (operand bit planes padded to 64)
 UNIT = "pairs/s"
@@ -324,7 +327,8 @@ def main() -> None:
         for r in red_sweep:
             per_pattern[r["pattern"]] = max(per_pattern.get(r["pattern"], 0.0), r["adds_per_s"])
         roofline = {"bound": "shared_atomic", "achieved": per_gpu * apr / 1e9, "peak": red_peak / 1e9,
-                    "unit": "Gred/s", "frac": per_gpu * apr / red_peak, "traffic": NCU_DRAM_BYTES_PER_LAUNCH_MMA,
+                    "unit": "Gred/s", "frac": per_gpu * apr / red_peak,
+                    "traffic": NCU_DRAM_BYTES_PER_LAUNCH_MMA["paired" if paired else "single"],
                     "traffic_source": "dram__bytes_read.sum + dram__bytes_write.sum of one mma_hist_kernel launch, "
                                       "ncu capture at k=20; operands are generated "
                                       "on chip, so the figure does not grow with k",
@@ -341,7 +345,7 @@ def main() -> None:
                     "tensor_pipe": {"achieved_tops": per_gpu * 2 * k_per_pair / 1e12,
                                     "peak_tops": INT8_DENSE_TOPS_NOMINAL, "peak_source": "nominal dense int8",
                                     "frac": per_gpu * 2 * k_per_pair / 1e12 / INT8_DENSE_TOPS_NOMINAL,
-                                    "ncu_tensor_cycles_active_pct": NCU_TENSOR_PIPE_PCT_MMA}}
+                                    "ncu_tensor_cycles_active_pct": NCU_TENSOR_PIPE_PCT_MMA["paired" if paired else "single"]}}
     else:
         achieved_popc = per_gpu * 1.0  # one 32-bit POPC per pair (high word folded per segment)
         roofline = {"bound": "popc", "achieved": achieved_popc / 1e9, "peak": popc_peak / 1e9, "unit": "Gpopc/s",

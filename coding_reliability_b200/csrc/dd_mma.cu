@@ -89,13 +89,16 @@ constexpr uint32_t kMinSmem = 120 * 1024;  // more than half an SM: one CTA (and
 constexpr unsigned long long kDrainTimeoutNs = 2000000000ull;
 constexpr int kBufs = kTmemCols / kN;   // accumulator buffers
 // Pauses (ns) between the polls of a waiting epilogue warp (for its next tile),
-// of the issuer (for a free accumulator buffer) and of the generators (for a free
-// operand slot).  A poll is a shared-memory pipe operation, as is every binning
-// atomic: 400 ns for the epilogue measured best (k=22: 5.96e12 pairs/s without a
-// pause, 6.09e12 at 120 ns, 6.14e12 at 400 ns, 6.03e12 at 1000 ns); a pause for
-// the issuer changed nothing.
-constexpr unsigned kEpiPollNs = 400;
-constexpr unsigned kIssuerPollNs = 0;
+// of the issuer (for a free accumulator buffer or the next strip's operands) and
+// of the generators (for a free operand slot).  A poll is a shared-memory pipe
+// operation, as is every binning atomic, and an issue slot taken from the
+// epilogue warps of the same scheduler.  Single epilogue, k=22: 5.96e12 pairs/s
+// without an epilogue pause, 6.09e12 at 120 ns, 6.14e12 at 400 ns, 6.03e12 at
+// 1000 ns.  Paired epilogue, whose binning is issue-bound, k=22: issuer 8.77e12
+// without a pause, 9.06-9.08e12 at 64-500 ns; then epilogue 8.95e12 at 100 ns,
+// 9.02e12 at 400 ns, 9.11e12 at 800 ns, 9.02e12 at 1600 ns; generators 200 ns: -1 %.
+constexpr unsigned kEpiPollNs = 800;
+constexpr unsigned kIssuerPollNs = 200;
 constexpr unsigned kGenPollNs = 0;
 constexpr int kColsPerWarp = kN / (kEpiWarps / 4);  // columns of a tile each epilogue warp reads
 constexpr int kLoads = kColsPerWarp / 32;           // 32-column TMEM loads per warp and tile
@@ -608,7 +611,8 @@ __global__ void __launch_bounds__(kThreads, 1) mma_hist_kernel(MmaArgs args) {
       };
       for (uint64_t s = 0;; ++s) {
         const uint32_t slot = (uint32_t)(s & 1);
-        if (!wait_or_abort(smem_u32(&sh->slot_full[slot]), (uint32_t)(s >> 1) & 1u, args.timeout_ns, abort)) break;
+        if (!wait_or_abort<kIssuerPollNs>(smem_u32(&sh->slot_full[slot]), (uint32_t)(s >> 1) & 1u, args.timeout_ns, abort))
+          break;
         const StripInfo si = sh->strip[slot];
         if (si.flags & kInfoDone) { normal = true; break; }
         const uint32_t a0 = smem_u32(sA + slot * kABytes);

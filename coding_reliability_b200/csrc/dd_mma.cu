@@ -107,7 +107,7 @@ static_assert(kEpiWarps % 4 == 0 && kColsPerWarp % 32 == 0, "whole 32-column TME
 // tile order share their column operand (written once per claim and column).
 constexpr int kClaimStrips = 4 * kStrips;
 // pair-packed epilogue
-constexpr int kPkHalf = kSuper / 2;                 // column p of a strip pairs with column p + 512
+constexpr int kPkHalf = kSuper / 2;                 // packed columns of a strip: p holds columns 2p, 2p + 1
 constexpr int kPkTilesPerStrip = kPkHalf / kN;      // 2 MMA tiles of 256 packed columns per strip
 constexpr int kPkBBytes = kPkTilesPerStrip * kBTileBytes;  // 32 KB column operand per super tile
 constexpr uint32_t kPkFb = 64;                      // fallback row after the joint cells: single distances 0..63
@@ -566,10 +566,11 @@ __global__ void __launch_bounds__(kThreads, 1) mma_hist_kernel(MmaArgs args) {
         uint8_t* bb = sB + (size_t)bcur * kColBytes;
         const uint64_t ncols = rect ? NC : N;
         if constexpr (kPk) {
-          // packed column p: columns c0 + p and c0 + p + 512 of the super tile
+          // packed column p: the adjacent columns c0 + 2p and c0 + 2p + 1, so a
+          // diagonal or edge strip has few packed values with just one valid pair
 #pragma unroll 1
           for (int cc = gtid; cc < kPkHalf; cc += kGenThreads) {
-            const uint64_t j = c0 + cc, j2 = j + kPkHalf;
+            const uint64_t j = c0 + 2 * (uint64_t)cc, j2 = j + 1;
             write_col_pk(bb + (cc / kN) * kBTileBytes, cc % kN, j < ncols ? mma_col_value(jp, j) : 0,
                          j2 < ncols ? mma_col_value(jp, j2) : 0, L, S, lo);
           }
@@ -803,21 +804,27 @@ __global__ void __launch_bounds__(kThreads, 1) mma_hist_kernel(MmaArgs args) {
           }
         } else {
           // partial strip: every pair checked; a value whose two pairs both count
-          // and whose d2 lies in the window still takes one joint cell.  The
-          // strip's entry stays valid while its tiles are binned: the issuer
+          // and whose d2 lies in the window still takes one joint cell.  Value u
+          // holds columns cbase + 2u and cbase + 2u + 1: a pair counts when its
+          // row is a row of the job and its column offset o in [0, 64) satisfies
+          // lo_o < o < hi_o (triangle: the column lies above the row's diagonal
+          // and inside the job; grid: inside the job), bounds clamped to 32 bits.
+          // The strip's entry stays valid while its tiles are binned: the issuer
           // rewrites it for strip s+4 only after every warp has released the
           // tiles of strip s+3.  (Kept inline: a non-inlined copy of this loop,
-          // fed through a local array, measured slower, e.g. the k=16 sweep
-          // 5.8e12 -> 4.9e12 pairs/s.)
+          // fed through a local array, measured slower.)
           const StripInfo& es = sh->estrip[(g / kTps) & 3];
-          const uint64_t n_ = es.n, nc_ = es.cols;
           const uint64_t i = es.r0 + (uint64_t)(q * 32 + lane);
-          const uint64_t j0 = es.c0 + (g % kTps) * (uint64_t)kN + (uint64_t)(sub * kColsPerWarp + 32 * h);
+          const uint64_t cbase = es.c0 + 2 * ((g % kTps) * (uint64_t)kN + (uint64_t)(sub * kColsPerWarp + 32 * h));
+          const bool rect = (flags & kInfoRect) != 0;
+          const int64_t dlo = rect ? -1 : (int64_t)i - (int64_t)cbase;            // o > dlo
+          const int64_t dhi = (int64_t)(rect ? es.cols : es.n) - (int64_t)cbase;  // o < dhi
+          const int32_t lo_o = i < es.n ? (int32_t)(dlo < -1 ? -1 : (dlo > 64 ? 64 : dlo)) : 64;
+          const int32_t hi_o = (int32_t)(dhi < 0 ? 0 : (dhi > 64 ? 64 : dhi));
 #pragma unroll
           for (int u = 0; u < 32; ++u) {
-            const uint64_t j = j0 + u, j2 = j + kPkHalf;
-            const bool v1 = (flags & kInfoRect) ? (i < n_ && j < nc_) : (i < n_ && j < n_ && j > i);
-            const bool v2 = (flags & kInfoRect) ? (i < n_ && j2 < nc_) : (i < n_ && j2 < n_ && j2 > i);
+            const bool v1 = 2 * u > lo_o && 2 * u < hi_o;
+            const bool v2 = 2 * u + 1 > lo_o && 2 * u + 1 < hi_o;
             if (v1 && v2 && x[u] < pklimit) red_shared(pk_lane + (x[u] << 7));
             else if (v1 || v2) pk_single(x[u], v1, v2);
           }

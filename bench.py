@@ -46,8 +46,8 @@ NCU_DRAM_BYTES_PER_LAUNCH = 108288  # popc path: DRAM bytes of one launch, ncu c
 # tcgen05 path, by epilogue: DRAM bytes of one launch and sm__pipe_tensor_cycles_active
 # of an ncu capture at k=20 (cold caches: the bytes are the job table, the bins and the
 # kernel's own code; codewords are generated on chip)
-NCU_DRAM_BYTES_PER_LAUNCH_MMA = {"paired": 206848, "single": 81408}
-NCU_TENSOR_PIPE_PCT_MMA = {"paired": 11.5, "single": 16.9}
+NCU_DRAM_BYTES_PER_LAUNCH_MMA = {"paired": 136448, "single": 81408}
+NCU_TENSOR_PIPE_PCT_MMA = {"paired": 12.1, "single": 16.9}
 INT8_DENSE_TOPS_NOMINAL = 4500.0  # B200 dense int8 tensor rate (nominal; the measured peaks cover bf16 only)
 MMA_K_PAD = 64  # int8 K of every tcgen05 tile (operand bit planes padded to 64)
 UNIT = "pairs/s"

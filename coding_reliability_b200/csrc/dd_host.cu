@@ -114,13 +114,23 @@ static uint32_t mma_epilogue_of(const dd_context* ctx) {
   return ctx->mma_epilogue == DD_MMA_EPILOGUE_AUTO ? ctx->mma_tuned_epilogue : ctx->mma_epilogue;
 }
 
+// Jobs below this many distance evaluations stay on the popc kernel under
+// AUTO: the tcgen05 kernel's fixed cost per launch (TMEM allocation, clearing
+// its ~180 KB of shared-memory table, barrier set-up) outweighs its rate there
+// (A = 641, k = 12, 8.4e6 pairs: popc 0.09 ms, tcgen05 0.44 ms; k = 16, 2.1e9
+// pairs, one launch each: tcgen05 0.41 ms, popc 0.57 ms).
+constexpr double kMmaMinPairs = 1073741824.0;  // 2^30
+
 // Which kernel runs a job: explicit MMA or POPC requests are honoured where
-// the job allows them; AUTO uses the context's measured preference.
+// the job allows them; AUTO uses the context's measured preference for jobs
+// large enough to amortise the tcgen05 kernel's launch.
 static bool want_mma(const dd_context* ctx, const Job& j, uint32_t kernel) {
   if (!mma_eligible(j)) return false;
   if (kernel == DD_KERNEL_MMA) return true;
   if (kernel == DD_KERNEL_POPC) return false;
-  return ctx->tuned == 2;  // autotuner's verdict for AN exhaustive shapes
+  const double pairs = j.shape == SHAPE_TRIANGLE ? 0.5 * (double)j.rows * (double)j.rows
+                                                 : (double)j.rows * (double)j.cols;
+  return ctx->tuned == 2 && pairs >= kMmaMinPairs;  // autotuner's verdict for AN exhaustive shapes
 }
 
 // Orders the job table (popc jobs first, then MMA jobs), assigns tile ranges

@@ -68,7 +68,8 @@ typedef enum dd_mode {
  * Ext-Hamming all-pairs brute force (Monte Carlo, the Ext-Hamming weight
  * enumerator and anything wider than 60-bit operands use the popc kernel). */
 typedef enum dd_kernel {
-  DD_KERNEL_AUTO = 0,  /* autotuner's choice for the shape */
+  DD_KERNEL_AUTO = 0,  /* autotuner's choice for the shape; jobs below 2^30 pairs stay on the popc
+                          kernel, whose launch costs less than the tcgen05 kernel's fixed set-up */
   DD_KERNEL_POPC = 1,  /* XOR + POPC, warp-private shared-memory bins */
   DD_KERNEL_MMA = 2    /* tcgen05 kind::i8 bit-plane MMA, histogram epilogue from TMEM */
 } dd_kernel;

@@ -36,3 +36,28 @@ def test_percentile_is_nearest_rank():
     assert bench.percentile(v, 0.99) == 48.0
     assert bench.percentile([5.0], 0.99) == 5.0
     assert bench.percentile(sorted(float(x) for x in range(1, 101)), 0.99) == 99.0
+
+
+class _StandIn:
+    """A context stand-in that returns a fixed histogram for either kernel."""
+    def __init__(self, raw, counts, differ=False):
+        self.raw, self.counts, self.differ = raw, counts, differ
+
+    def histogram(self, req):
+        import types
+        counts = list(self.counts)
+        if self.differ:
+            counts[1] += 1
+        return types.SimpleNamespace(kernel_used=req.kernel, raw=list(self.raw), counts=counts, kernel_ms=1000.0)
+
+
+def test_cross_kernel_check_requires_identical_histograms():
+    import types
+    timed = types.SimpleNamespace(kernel_used=dd.KERNEL_MMA, raw=[0, 3, 5], counts=[8, 6, 10])
+    out = bench.cross_kernel_check(_StandIn(timed.raw, timed.counts), dd, 641, 3, timed)
+    assert out["cross_kernel"] and out["other_kernel"] == "popc" and out["timed_kernel"] == "mma"
+    assert out["sha256_counts"] == bench.counts_digest([8, 6, 10])
+    assert out["other_kernel_pairs_per_s"] == bench.pairs_of(3) / 1.0
+    import pytest
+    with pytest.raises(AssertionError):
+        bench.cross_kernel_check(_StandIn(timed.raw, timed.counts, differ=True), dd, 641, 3, timed)

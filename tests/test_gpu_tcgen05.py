@@ -139,3 +139,27 @@ def test_mma_hamming_reference_runs(ctx, epi):
                                        kernel=dd.KERNEL_MMA))
         on_mma(res, epi)
         assert res.counts == run["counts"], args
+
+
+def test_mma_batch_mixed_shapes(ctx, epi):
+    """One launch over jobs of different widths: windowed jobs (A = 58659, k = 18..20:
+    S = 35..37, the joint table holds only part of the d2 rows) beside jobs whose
+    window holds every distance (small k), a 1-D grid and an Ext-Hamming all-pairs job.
+    The table is folded with each job's own S and window at every job change; every
+    histogram equals its popc-kernel run."""
+    reqs = [dd.Request(dd.CODE_AN, dd.MODE_EXHAUSTIVE, 58659, 20, kernel=dd.KERNEL_MMA),
+            dd.Request(dd.CODE_AN, dd.MODE_EXHAUSTIVE, 641, 12, kernel=dd.KERNEL_MMA),
+            dd.Request(dd.CODE_AN, dd.MODE_EXHAUSTIVE, 58659, 18, kernel=dd.KERNEL_MMA),
+            dd.Request(dd.CODE_AN, dd.MODE_EXHAUSTIVE, 61, 14, kernel=dd.KERNEL_MMA),
+            dd.Request(dd.CODE_AN, dd.MODE_GRID_1D, 1021, 20, m=4096, kernel=dd.KERNEL_MMA),
+            dd.Request(dd.CODE_AN, dd.MODE_EXHAUSTIVE, 32771, 19, kernel=dd.KERNEL_MMA),
+            dd.Request(dd.CODE_EXT_HAMMING, dd.MODE_EXHAUSTIVE, 1, 16, hamming_method=dd.HAMMING_ALL_PAIRS,
+                       kernel=dd.KERNEL_MMA)]
+    for graph in (False, True):
+        out = ctx.batch(reqs, use_graph=graph, kernel=dd.KERNEL_MMA)
+        for q, r in zip(reqs, out):
+            on_mma(r, epi)
+            p = dd.Request(q.code, q.mode, q.A, q.n, m=q.m, hamming_method=q.hamming_method, kernel=dd.KERNEL_POPC)
+            s = ctx.histogram(p)
+            assert s.kernel_used == dd.KERNEL_POPC
+            assert r.raw == s.raw and r.counts == s.counts, q

@@ -12,20 +12,25 @@
 // shared-memory bin per pair (per-thread bin columns).
 //
 // Pair-packed (two distances per MMA column): column p carries two codewords y
-// and y' (columns j and j + 512 of the strip), with S = largest distance + 1:
+// and y' (the adjacent columns 2p and 2p + 1 of the strip), with S = largest
+// distance + 1:
 //   A row i:    bytes k<L: -2*b_ik;            byte L: popc(x_i); byte L+1: S;              byte L+2: 1
 //   B column p: bytes k<L: b_yk + S*b_y'k;     byte L: 1 + S;     byte L+1: popc(y') - lo;  byte L+2: popc(y)
 // so D[i][p] = d(x_i, y) + S*(d(x_i, y') - lo), every byte within int8.  That
-// value is directly the cell of a joint (d1, d2) table of 1024 cells whenever
-// d2 lies in the window [lo, lo + 1024/S) chosen on the host from the job's
-// distance distribution: one shared-memory atomic counts two pairs.  The OR of
-// a tile's values shows at once whether any lies outside [0, 1024); only then
-// are values checked one by one and the outliers counted as two single
-// distances in a fallback row.  The table has one column per lane, shared by
-// all epilogue warps, and is folded into the job's bins (row sums for d2,
-// column sums for d1) when the job changes, every kPkFlushTiles tiles and at
-// exit, between two bounded epilogue-wide barriers.  It also halves the MMAs,
-// tensor-memory loads and column-operand bytes per pair.
+// value is directly the cell of a joint (d1, d2) table whenever d2 lies in the
+// job's window [lo, lo + rows): the table holds as many whole rows of S cells as
+// fit in shared memory (mma_pk_layout), and the host places the window on the
+// job's distance distribution (mma_pack_setup).  One shared-memory atomic then
+// counts two pairs.  The unsigned maximum of 32 values against S * rows shows
+// at once whether any lies outside the window (a d2 below it gives a negative,
+// i.e. huge, value); only then are the values checked one by one and the
+// outliers counted as two single distances in a fallback row.  A job whose
+// window holds every d2 (lo = 0, rows = S) skips the test.  The table has one
+// column per lane, shared by all epilogue warps, and is folded into the job's
+// bins (row sums for d2, column sums for d1) when the job changes, every
+// kPkFlushTiles tiles and at exit, between two bounded epilogue-wide barriers.
+// It also halves the MMAs, tensor-memory loads and column-operand bytes per
+// pair.
 //
 // Work unit: the popc kernel's tile space (1024x1024 super tiles of the i<j
 // triangle, column by column, split into 8 strips of 128 rows; for grid jobs,

@@ -196,6 +196,7 @@ def load() -> C.CDLL:
     lib.dd_server_poll.argtypes = [vp, C.c_uint64, C.POINTER(_Res), C.POINTER(C.c_int)]
     lib.dd_server_wait.argtypes = [vp, C.c_uint64, C.c_double, C.POINTER(_Res)]
     lib.dd_server_cancel.argtypes = [vp, C.c_uint64]
+    lib.dd_server_release.argtypes = [vp, C.c_uint64]
     lib.dd_server_get_stats.argtypes = [vp, C.c_void_p]
     lib.dd_server_shutdown.argtypes = [vp]
     lib.dd_server_destroy.argtypes = [vp]
@@ -498,6 +499,15 @@ class Server:
         h = self._enter()
         try:
             _check(load().dd_server_cancel(h, ticket))
+        finally:
+            self._leave()
+
+    def release(self, ticket: int) -> None:
+        """Drops a finished query's result now (DDError 6 while it runs or is waited on).
+        Delivered results are also dropped by themselves once 4096 newer ones were delivered."""
+        h = self._enter()
+        try:
+            _check(load().dd_server_release(h, ticket))
         finally:
             self._leave()
 

@@ -12,6 +12,14 @@
 // while a round runs are admitted at the next round, so large and small
 // queries overlap on the device and a small one never waits for a large one
 // to finish.
+//
+// Host memory stays bounded for a long-running server: a finished query's
+// record (its result) is kept until the result has been delivered (a wait
+// that returned it, a poll that reported it done, or the query was cancelled
+// by its client); the last kKeepDelivered delivered records stay answerable,
+// older ones are dropped (never while a thread waits on them), and
+// dd_server_release drops one at once.  Latency percentiles cover the last
+// kLatencyWindow completed queries.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -39,6 +47,8 @@ double now_ms() {
 }
 
 constexpr uint64_t kSlotBytes = dd::kMaxBins * 8 + sizeof(dd::Job) + 16;  // bins + job entry + cursor
+constexpr size_t kKeepDelivered = 4096;   // delivered results that stay answerable
+constexpr size_t kLatencyWindow = 65536;  // completed queries behind p50 / p99
 
 struct Query {
   uint64_t ticket = 0;
@@ -50,6 +60,8 @@ struct Query {
   int slot = -1;
   bool cancelled = false;
   bool done = false;
+  bool delivered = false; // its result reached the client (or the client cancelled it)
+  int waiters = 0;        // threads inside dd_server_wait on this query: it is not dropped meanwhile
   double t_submit = 0;
   dd_result result{};     // zero until the query finishes
 };
@@ -83,7 +95,9 @@ struct dd_server {
   uint64_t submitted = 0, admitted = 0, completed = 0, rejected = 0, cancelled = 0, rounds = 0;
   double busy_ms = 0;
   u128 pairs_done = 0;
-  std::vector<double> latencies;
+  std::vector<double> latencies;  // ring of the last kLatencyWindow completions
+  size_t latency_next = 0;
+  std::deque<uint64_t> delivered;  // delivered records, oldest first
 };
 
 namespace {
@@ -99,6 +113,22 @@ struct Inside {
   Inside& operator=(const Inside&) = delete;
 };
 
+// Records that q's result reached its client; drops the oldest delivered
+// records beyond kKeepDelivered (skipping any a thread still waits on).
+void note_delivered(dd_server* s, Query& q) {
+  if (q.delivered) return;
+  q.delivered = true;
+  s->delivered.push_back(q.ticket);
+  for (size_t tries = s->delivered.size(); s->delivered.size() > kKeepDelivered && tries > 0; --tries) {
+    const uint64_t t = s->delivered.front();
+    s->delivered.pop_front();
+    auto it = s->queries.find(t);
+    if (it == s->queries.end()) continue;
+    if (it->second.waiters > 0) { s->delivered.push_back(t); continue; }
+    s->queries.erase(it);
+  }
+}
+
 void finish(dd_server* s, Query& q, int status) {
   q.done = true;
   q.result.status = (uint32_t)status;
@@ -109,7 +139,9 @@ void finish(dd_server* s, Query& q, int status) {
   q.result.total_ms = now_ms() - q.t_submit;
   if (status == DD_OK) {
     s->completed++;
-    s->latencies.push_back(q.result.total_ms);
+    if (s->latencies.size() < kLatencyWindow) s->latencies.push_back(q.result.total_ms);
+    else s->latencies[s->latency_next] = q.result.total_ms;
+    s->latency_next = (s->latency_next + 1) % kLatencyWindow;
     s->pairs_done += q.pairs;
   } else if (status == DD_ERR_CANCELLED) {
     s->cancelled++;
@@ -118,6 +150,7 @@ void finish(dd_server* s, Query& q, int status) {
     s->free_slots.push_back(q.slot);
     q.slot = -1;
   }
+  if (q.cancelled) note_delivered(s, q);  // its client went away (or asked for the status, which stays)
   s->cv_done.notify_all();
 }
 
@@ -301,7 +334,10 @@ int dd_server_poll(dd_server* s, uint64_t ticket, dd_result* res, int* done) {
   auto it = s->queries.find(ticket);
   if (it == s->queries.end()) { dd::set_error("unknown ticket"); return DD_ERR_NOT_FOUND; }
   *done = it->second.done ? 1 : 0;
-  if (it->second.done && res) *res = it->second.result;
+  if (it->second.done && res) {
+    *res = it->second.result;
+    note_delivered(s, it->second);
+  }
   return DD_OK;
 }
 
@@ -311,14 +347,22 @@ int dd_server_wait(dd_server* s, uint64_t ticket, double timeout_s, dd_result* r
   Inside in(s);
   auto it = s->queries.find(ticket);
   if (it == s->queries.end()) { dd::set_error("unknown ticket"); return DD_ERR_NOT_FOUND; }
-  auto ready = [&] { return s->queries[ticket].done; };
+  // the record stays put while waiters > 0 (references into the map survive rehashing)
+  Query* q = &it->second;
+  q->waiters++;
+  auto ready = [q] { return q->done; };
+  bool finished = true;
   if (timeout_s < 0) s->cv_done.wait(lk, ready);
-  else if (!s->cv_done.wait_for(lk, std::chrono::duration<double>(timeout_s), ready)) {
+  else finished = s->cv_done.wait_for(lk, std::chrono::duration<double>(timeout_s), ready);
+  q->waiters--;
+  if (!finished) {
     dd::set_error("query still running");
     return DD_ERR_TIMEOUT;
   }
-  if (res) *res = s->queries[ticket].result;
-  return (int)s->queries[ticket].result.status;
+  if (res) *res = q->result;
+  const int st = (int)q->result.status;
+  note_delivered(s, *q);  // may drop older records, never this one's reference before here
+  return st;
 }
 
 int dd_server_cancel(dd_server* s, uint64_t ticket) {
@@ -335,6 +379,22 @@ int dd_server_cancel(dd_server* s, uint64_t ticket) {
     s->queue.erase(qi);
     finish(s, q, DD_ERR_CANCELLED);
   }
+  return DD_OK;
+}
+
+int dd_server_release(dd_server* s, uint64_t ticket) {
+  if (!s) { dd::set_error("NULL argument"); return DD_ERR_INVALID_ARGUMENT; }
+  std::lock_guard<std::mutex> lk(s->mu);
+  Inside in(s);
+  auto it = s->queries.find(ticket);
+  if (it == s->queries.end()) { dd::set_error("unknown ticket"); return DD_ERR_NOT_FOUND; }
+  if (!it->second.done) { dd::set_error("query still running (cancel it and wait first)"); return DD_ERR_BUSY; }
+  if (it->second.waiters > 0) { dd::set_error("threads are waiting on this query"); return DD_ERR_BUSY; }
+  if (it->second.delivered) {
+    auto d = std::find(s->delivered.begin(), s->delivered.end(), ticket);
+    if (d != s->delivered.end()) s->delivered.erase(d);
+  }
+  s->queries.erase(it);
   return DD_OK;
 }
 
@@ -359,9 +419,9 @@ int dd_server_get_stats(dd_server* s, dd_server_stats* out) {
   out->pairs_per_s = s->busy_ms > 0 ? (double)s->pairs_done / (s->busy_ms * 1e-3) : 0.0;
   if (!s->latencies.empty()) {
     std::vector<double> v = s->latencies;
-    std::sort(v.begin(), v.end());
-    auto pct = [&](double p) {
-      const size_t i = (size_t)std::min<double>((double)v.size() - 1, std::ceil(p * v.size()) - 1);
+    auto pct = [&](double p) {  // nearest rank
+      const size_t i = (size_t)std::max(0.0, std::min<double>((double)v.size() - 1, std::ceil(p * v.size()) - 1));
+      std::nth_element(v.begin(), v.begin() + (std::ptrdiff_t)i, v.end());
       return v[i];
     };
     out->p50_ms = pct(0.50);

@@ -254,7 +254,7 @@ typedef struct dd_server_options {
 typedef struct dd_server_stats {
   uint64_t submitted, admitted, completed, rejected, cancelled, rounds;
   uint32_t active, queued, slots, slots_free;
-  double p50_ms, p99_ms;        /* latency from submit to result, completed queries */
+  double p50_ms, p99_ms;        /* latency from submit to result, the last 65536 completed queries */
   double pairs_per_s;           /* distance evaluations of completed queries / busy device time */
   double busy_ms;               /* device time of all rounds */
   uint64_t pairs_lo, pairs_hi;  /* distance evaluations of completed queries (uint128) */
@@ -267,6 +267,13 @@ int dd_server_submit(dd_server* s, const dd_request* req, uint64_t* ticket);
 int dd_server_poll(dd_server* s, uint64_t ticket, dd_result* res, int* done);
 /* Blocks up to timeout_s seconds (< 0: no limit); DD_ERR_TIMEOUT if still running. */
 int dd_server_wait(dd_server* s, uint64_t ticket, double timeout_s, dd_result* res);
+/* Result retention: a finished query's result is kept until it has been delivered
+ * (dd_server_wait returned it, dd_server_poll reported it done with a result
+ * buffer, or its client cancelled it); the 4096 most recently delivered results
+ * stay answerable, older ones are dropped (never while a thread waits on them)
+ * and their tickets then give DD_ERR_NOT_FOUND.  dd_server_release drops a
+ * finished query's result at once (DD_ERR_BUSY while it runs or is waited on). */
+int dd_server_release(dd_server* s, uint64_t ticket);
 /* A client that goes away: a queued query is dropped, an active one stops after
  * the current round and frees its slot; its result status is DD_ERR_CANCELLED. */
 int dd_server_cancel(dd_server* s, uint64_t ticket);

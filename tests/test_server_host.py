@@ -166,3 +166,33 @@ def test_many_clients_latency_stats(lib):
         assert st["completed"] == 40 and st["submitted"] == 40
         assert 0 < st["p50_ms"] <= st["p99_ms"]
         assert st["slots_free"] == st["slots"]
+
+
+def test_release_and_retention(lib):
+    """A delivered result stays answerable until 4096 newer ones were delivered,
+    then its ticket is unknown; release drops a finished one at once and refuses
+    a running one."""
+    with dd.Server(dry_run=True, round_ms=1) as s:
+        t_big = s.submit(big())
+        until(lambda: s.stats()["active"] == 1)
+        with pytest.raises(dd.DDError) as e:
+            s.release(t_big)  # still running
+        assert e.value.status == 6
+        t = s.submit(small())
+        assert s.wait(t, 10)[0] == 0
+        assert s.wait(t, 10)[0] == 0  # delivered results stay answerable
+        s.release(t)
+        with pytest.raises(dd.DDError) as e:
+            s.poll(t)
+        assert e.value.status == 8
+        tickets = [s.submit(small(A=2 * i + 33, n=8)) for i in range(4100)]
+        for x in tickets:
+            assert s.wait(x, 10)[0] == 0
+        with pytest.raises(dd.DDError) as e:  # the oldest delivered records were dropped
+            s.poll(tickets[0])
+        assert e.value.status == 8
+        assert s.poll(tickets[-1]) is not None
+        s.cancel(t_big)
+        assert s.wait(t_big, 10)[0] == 9
+        st = s.stats()
+        assert st["completed"] == 4101 and 0 < st["p50_ms"] <= st["p99_ms"]

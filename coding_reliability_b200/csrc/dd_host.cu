@@ -49,6 +49,8 @@ struct dd_context {
   std::vector<dd::Job> gjobs;  // job table the cached graph was built for
   int ggrid[2] = {0, 0};
   size_t gsmem[2] = {0, 0};
+  int ghist_mode = 0;                  // popc bin-increment form the graph launches
+  unsigned long long gtimeout_ns = 0;  // device-side wait bound baked into the graph
 };
 
 namespace dd {
@@ -68,8 +70,18 @@ static int cuda_fail(cudaError_t e, const char* what) {
     if (e_ != cudaSuccess) return cuda_fail(e_, #call); \
   } while (0)
 
+// The cached launch graph's copy nodes and kernel arguments point at these
+// buffers, so it is dropped whenever one of them is reallocated (no graph is in
+// flight here: every launch is synchronised before its call returns).
+static void drop_graph(dd_context* ctx) {
+  if (ctx->gexec) cudaGraphExecDestroy(ctx->gexec);
+  ctx->gexec = nullptr;
+  ctx->gjobs.clear();
+}
+
 static int ensure_capacity(dd_context* ctx, uint32_t slots, uint32_t njobs) {
   DD_CUDA(cudaSetDevice(ctx->device));
+  if (slots > ctx->bin_slots || njobs > ctx->job_cap) drop_graph(ctx);
   if (slots > ctx->bin_slots) {
     if (ctx->d_bins) cudaFree(ctx->d_bins);
     if (ctx->h_bins) cudaFreeHost(ctx->h_bins);
@@ -340,9 +352,11 @@ int dd_context_create(int device, void* stream, dd_context** out) {
   cudaError_t e = cudaSetDevice(device);
   if (e == cudaSuccess) e = cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, device);
   if (e == cudaSuccess) {
-    int major = 0;
+    // sm_100a code is arch-specific: it runs on compute capability 10.0 only
+    int major = 0, minor = 0;
     cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, device);
-    if (major != 10) {
+    cudaDeviceGetAttribute(&minor, cudaDevAttrComputeCapabilityMinor, device);
+    if (major != 10 || minor != 0) {
       delete ctx;
       set_error("this library is built for sm_100a (B200) only");
       return DD_ERR_NO_DEVICE;
@@ -484,9 +498,10 @@ static int run_requests(dd_context* ctx, const dd_request* reqs, uint32_t count,
     const size_t nj = lp.npopc + lp.nmma;
     const bool same = ctx->gexec && ctx->gjobs.size() == nj && ctx->ggrid[0] == lp.pgrid &&
                       ctx->ggrid[1] == lp.mgrid && ctx->gsmem[0] == lp.psmem && ctx->gsmem[1] == lp.msmem &&
+                      ctx->ghist_mode == ctx->hist_mode && ctx->gtimeout_ns == lp.margs.timeout_ns &&
                       std::memcmp(ctx->gjobs.data(), ctx->h_jobs, nj * sizeof(Job)) == 0;
     if (!same) {
-      if (ctx->gexec) { cudaGraphExecDestroy(ctx->gexec); ctx->gexec = nullptr; }
+      drop_graph(ctx);
       cudaGraph_t g = nullptr;
       DD_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
       st = enqueue_launch(ctx, lp, true);
@@ -499,6 +514,8 @@ static int run_requests(dd_context* ctx, const dd_request* reqs, uint32_t count,
       ctx->gjobs.assign(ctx->h_jobs, ctx->h_jobs + nj);
       ctx->ggrid[0] = lp.pgrid; ctx->ggrid[1] = lp.mgrid;
       ctx->gsmem[0] = lp.psmem; ctx->gsmem[1] = lp.msmem;
+      ctx->ghist_mode = ctx->hist_mode;
+      ctx->gtimeout_ns = lp.margs.timeout_ns;
     }
     DD_CUDA(cudaGraphLaunch(ctx->gexec, s));
   } else {

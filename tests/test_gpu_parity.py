@@ -309,6 +309,22 @@ def test_batch_equals_single(ctx, kernel):
             assert r.counts == s.counts and r.raw == s.raw and r.minb == s.minb
 
 
+def test_graph_cache_after_buffer_growth(kernel):
+    """A fresh context replays a graph-captured batch after a larger batch has
+    reallocated its bins and job table: the cached graph is rebuilt for the new
+    buffers and gives the same histograms as the first run and as single runs."""
+    small = [an_req(A, 10) for A in range(33, 33 + 2 * 70, 2)]   # 70 requests: past the initial 64 slots
+    large = [an_req(A, 8) for A in range(33, 33 + 2 * 300, 2)]   # 300: grows the buffers again
+    with dd.Context(0) as c:
+        c.set_mma_epilogue(kernel.epilogue or dd.MMA_EPILOGUE_AUTO)
+        first = c.batch(small, use_graph=True, kernel=int(kernel))
+        c.batch(large, use_graph=True, kernel=int(kernel))
+        again = c.batch(small, use_graph=True, kernel=int(kernel))
+        assert [r.raw for r in again] == [r.raw for r in first]
+        for q, r in list(zip(small, again))[::7]:
+            assert r.raw == run(c, q, kernel).raw
+
+
 def test_super_a_sweep_k16_batched(ctx, kernel):
     """The 256-candidate k=16 sweep in one launch: every instance equals its own run,
     and the archived sweep pins (results/superAs/superA_n16_h16.txt) hold."""

@@ -31,21 +31,25 @@ constexpr int kOffset = 2;  // OFFSET, src/globals.cpp:24
 constexpr uint64_t kSeedAnMc = 16384;
 constexpr uint64_t kSeedHammingMc = 1337;
 
+// The drivers share one context on device 0.  A dd_context serves one host
+// thread at a time, so every call on it holds g_mu: drivers called from several
+// threads of a host application run one after the other.
 std::mutex g_mu;
 dd_context* g_ctx = nullptr;
 
-dd_context* shared_context() {
+template <class F>
+int on_shared_context(F&& f) {
   std::lock_guard<std::mutex> lk(g_mu);
   if (!g_ctx) {
     int st = dd_context_create(0, nullptr, &g_ctx);
     if (st != DD_OK) throw std::runtime_error(std::string("codrel_b200: ") + dd_last_error());
   }
-  return g_ctx;
+  return f(g_ctx);
 }
 
 dd_result run_request(const dd_request& req) {
   dd_result res;
-  int st = dd_histogram(shared_context(), &req, &res);
+  int st = on_shared_context([&](dd_context* c) { return dd_histogram(c, &req, &res); });
   if (st != DD_OK) throw std::runtime_error(std::string("codrel_b200: ") + dd_last_error());
   return res;
 }
@@ -268,7 +272,7 @@ double run_ancoding_mc_continue(uintll_t n, uintll_t iterations, uintll_t A, dou
   q.m = iterations;
   q.seed = kSeedAnMc;
   dd_result r;
-  int st = dd_mc_extend(shared_context(), &q, state.it_done, state.raw, &r);
+  int st = on_shared_context([&](dd_context* c) { return dd_mc_extend(c, &q, state.it_done, state.raw, &r); });
   if (st != DD_OK) throw std::runtime_error(std::string("codrel_b200: ") + dd_last_error());
   state.it_done = r.iterations;
   for (int b = 0; b < DD_MAX_BINS; ++b) state.raw[b] = r.raw[b];
@@ -395,7 +399,8 @@ void run_ancoding_batch(const uintll_t* As, const uint_t* hs, size_t count, Flag
   dd_batch_options opt;
   std::memset(&opt, 0, sizeof(opt));
   opt.use_graph = 1;
-  int st = dd_batch_run(shared_context(), reqs.data(), (uint32_t)count, res.data(), &opt);
+  int st = on_shared_context(
+      [&](dd_context* c) { return dd_batch_run(c, reqs.data(), (uint32_t)count, res.data(), &opt); });
   if (st != DD_OK) throw std::runtime_error(std::string("codrel_b200: ") + dd_last_error());
   for (size_t i = 0; i < count; ++i) {
     fill_counts(res[i], counts + i * DD_MAX_BINS);

@@ -48,6 +48,12 @@ NCU_DRAM_BYTES_PER_LAUNCH = 108288  # popc path: DRAM bytes of one launch, ncu c
 # kernel's own code; codewords are generated on chip)
 NCU_DRAM_BYTES_PER_LAUNCH_MMA = {"paired": 136448, "single": 81408}
 NCU_TENSOR_PIPE_PCT_MMA = {"paired": 12.1, "single": 16.9}
+# instruction issue, the bound of the tcgen05 path's epilogue: warp instructions per
+# pair (sm__inst_executed.sum / pairs of one k=20 launch; the single-epilogue capture
+# recorded no count) and smsp__issue_active of the same captures
+NCU_WARP_INST_PER_PAIR_MMA = {"paired": 5386.0 / 65536.0, "single": None}
+NCU_ISSUE_ACTIVE_PCT_MMA = {"paired": 64.1, "single": 65.2}
+ISSUE_PER_CLOCK_PER_SM = 4  # one warp instruction per clock from each of an SM's four schedulers
 INT8_DENSE_TOPS_NOMINAL = 4500.0  # B200 dense int8 tensor rate (nominal; the measured peaks cover bf16 only)
 MMA_K_PAD = 64  # int8 K of every tcgen05 tile (operand bit planes padded to 64)
 UNIT = "pairs/s"
@@ -346,6 +352,18 @@ def main() -> None:
                                     "peak_tops": INT8_DENSE_TOPS_NOMINAL, "peak_source": "nominal dense int8",
                                     "frac": per_gpu * 2 * k_per_pair / 1e12 / INT8_DENSE_TOPS_NOMINAL,
                                     "ncu_tensor_cycles_active_pct": NCU_TENSOR_PIPE_PCT_MMA["paired" if paired else "single"]}}
+        # and instruction issue, which bounds the epilogue
+        ipp = NCU_WARP_INST_PER_PAIR_MMA["paired" if paired else "single"]
+        sm_hz = (clk.get("sm_mhz") or 0) * 1e6
+        issue_peak = ISSUE_PER_CLOCK_PER_SM * torch.cuda.get_device_properties(local).multi_processor_count * sm_hz
+        roofline["issue"] = {
+            "warp_inst_per_pair": ipp,
+            "achieved_ginst_s": per_gpu * ipp / 1e9 if ipp else None,
+            "peak_ginst_s": issue_peak / 1e9 if issue_peak else None,
+            "frac": per_gpu * ipp / issue_peak if ipp and issue_peak else None,
+            "ncu_issue_active_pct": NCU_ISSUE_ACTIVE_PCT_MMA["paired" if paired else "single"],
+            "source": "warp instructions per pair from sm__inst_executed.sum of one k=20 ncu capture; peak = "
+                      "4 warp instructions per clock per SM at the median SM clock sampled in the timed region"}
     else:
         achieved_popc = per_gpu * 1.0  # one 32-bit POPC per pair (high word folded per segment)
         roofline = {"bound": "popc", "achieved": achieved_popc / 1e9, "peak": popc_peak / 1e9, "unit": "Gpopc/s",

@@ -59,6 +59,21 @@ MMA_K_PAD = 64  # int8 K of every tcgen05 tile (operand bit planes padded to 64)
 UNIT = "pairs/s"
 
 
+def issue_roofline(pairs_per_s: float, epilogue: str, sm_mhz, num_sms: int) -> dict:
+    """Instruction issue of the tcgen05 path (the bound of its epilogue): warp
+    instructions per pair from the ncu capture against 4 warp instructions per
+    clock per SM at the sampled SM clock.  Fields are None where a figure is missing."""
+    ipp = NCU_WARP_INST_PER_PAIR_MMA[epilogue]
+    peak = ISSUE_PER_CLOCK_PER_SM * num_sms * (sm_mhz or 0) * 1e6
+    return {"warp_inst_per_pair": ipp,
+            "achieved_ginst_s": pairs_per_s * ipp / 1e9 if ipp else None,
+            "peak_ginst_s": peak / 1e9 if peak else None,
+            "frac": pairs_per_s * ipp / peak if ipp and peak else None,
+            "ncu_issue_active_pct": NCU_ISSUE_ACTIVE_PCT_MMA[epilogue],
+            "source": "warp instructions per pair from sm__inst_executed.sum of one k=20 ncu capture; peak = "
+                      "4 warp instructions per clock per SM at the median SM clock sampled in the timed region"}
+
+
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
@@ -353,17 +368,8 @@ def main() -> None:
                                     "frac": per_gpu * 2 * k_per_pair / 1e12 / INT8_DENSE_TOPS_NOMINAL,
                                     "ncu_tensor_cycles_active_pct": NCU_TENSOR_PIPE_PCT_MMA["paired" if paired else "single"]}}
         # and instruction issue, which bounds the epilogue
-        ipp = NCU_WARP_INST_PER_PAIR_MMA["paired" if paired else "single"]
-        sm_hz = (clk.get("sm_mhz") or 0) * 1e6
-        issue_peak = ISSUE_PER_CLOCK_PER_SM * torch.cuda.get_device_properties(local).multi_processor_count * sm_hz
-        roofline["issue"] = {
-            "warp_inst_per_pair": ipp,
-            "achieved_ginst_s": per_gpu * ipp / 1e9 if ipp else None,
-            "peak_ginst_s": issue_peak / 1e9 if issue_peak else None,
-            "frac": per_gpu * ipp / issue_peak if ipp and issue_peak else None,
-            "ncu_issue_active_pct": NCU_ISSUE_ACTIVE_PCT_MMA["paired" if paired else "single"],
-            "source": "warp instructions per pair from sm__inst_executed.sum of one k=20 ncu capture; peak = "
-                      "4 warp instructions per clock per SM at the median SM clock sampled in the timed region"}
+        roofline["issue"] = issue_roofline(per_gpu, "paired" if paired else "single", clk.get("sm_mhz"),
+                                           torch.cuda.get_device_properties(local).multi_processor_count)
     else:
         achieved_popc = per_gpu * 1.0  # one 32-bit POPC per pair (high word folded per segment)
         roofline = {"bound": "popc", "achieved": achieved_popc / 1e9, "peak": popc_peak / 1e9, "unit": "Gpopc/s",

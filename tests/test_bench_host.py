@@ -1,6 +1,7 @@
 """Host-side pieces of bench.py that need no GPU: the serving mix covers every
 query class of the serving configuration (the k=32 grid included), and the
-latency percentiles are nearest-rank."""
+latency percentiles are nearest-rank, and the issue-rate roofline of the
+tcgen05 path."""
 import sys
 from pathlib import Path
 
@@ -61,3 +62,18 @@ def test_cross_kernel_check_requires_identical_histograms():
     import pytest
     with pytest.raises(AssertionError):
         bench.cross_kernel_check(_StandIn(timed.raw, timed.counts, differ=True), dd, 641, 3, timed)
+
+
+def test_issue_roofline():
+    """The tcgen05 path's issue figure: 5,386 warp instructions per 65,536-pair tile
+    (the ncu capture) at 9.35e12 pairs/s against 4 per clock on 148 SMs at 1965 MHz
+    is about 0.66; a missing clock or instruction count gives None, never an error."""
+    r = bench.issue_roofline(9.35e12, "paired", 1965.0, 148)
+    assert abs(r["warp_inst_per_pair"] - 5386 / 65536) < 1e-12
+    assert abs(r["peak_ginst_s"] - 4 * 148 * 1.965) < 1e-6
+    assert abs(r["frac"] - 0.6606) < 1e-3
+    assert r["achieved_ginst_s"] < r["peak_ginst_s"]
+    none_clock = bench.issue_roofline(9.35e12, "paired", None, 148)
+    assert none_clock["peak_ginst_s"] is None and none_clock["frac"] is None
+    single = bench.issue_roofline(6.1e12, "single", 1965.0, 148)
+    assert single["frac"] is None and single["ncu_issue_active_pct"] == 65.2

@@ -1,7 +1,7 @@
 """Host-side pieces of bench.py that need no GPU: the serving mix covers every
-query class of the serving configuration (the k=32 grid included), and the
-latency percentiles are nearest-rank, and the issue-rate roofline of the
-tcgen05 path."""
+query class of the serving configuration (the k=32 grid included), the latency
+percentiles are nearest-rank, and the tcgen05 path's issue-rate roofline is
+computed from the ncu figures and tolerates missing ones."""
 import sys
 from pathlib import Path
 
